@@ -1,0 +1,317 @@
+#!/usr/bin/env python
+"""Benchmark: colorings/sec of color-coding tree-template counting on B200.
+
+Default workload (N=1): the 12-vertex tree (path v0..v7, pendants v8@v2,
+v9@v4, v10@v5, v11@v10) on an R-MAT scale-20, edge-factor-8 graph
+(a,b,c = 0.57,0.19,0.19, seed 1; symmetrised, deduplicated), FP32 count
+tables, 16 colorings per step (coloring c seeded srand(7 + c)).
+
+  value     colorings/sec over all ranks, CUDA-event time of the counting
+            launches on the library's stream, inputs resident in HBM.
+  e2e       the same metric through the public C ABI per step: device graph
+            built from pinned host CSC arrays (H2D copy inside the timed
+            region), all colorings counted, raw counts read back (D2H).
+  roofline  the fused aggregation+eMA kernel: compulsory bytes per launch
+            divided by its CUDA-event duration, against MEASURED_PEAKS.json.
+  cpu_baseline  the reference's own CPU code (oracle/_ref/sc-nec-ncc.bin,
+            built from the reference sources) on the host cores.
+
+--impl reference runs that reference binary alone (rank 0) and prints its line.
+Multi-GPU (torchrun): every rank counts its own colorings of the same graph
+(independent replicas, weak scaling); the only exchange is the max of the
+step times and a gather of the counts.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+TEMPLATES = {
+    "p3": (3, [(0, 1), (1, 2)]),
+    "tree5": (5, [(0, 1), (1, 2), (2, 3), (1, 4)]),
+    "spider7": (7, [(0, 1), (1, 2), (0, 3), (3, 4), (0, 5), (5, 6)]),
+    "tree12": (12, [(0, 1), (1, 2), (2, 3), (3, 4), (4, 5), (5, 6), (6, 7), (2, 8), (4, 9), (5, 10), (10, 11)]),
+}
+WORKLOADS = {
+    # the 12-vertex tree on R-MAT scale 20, edge factor 8: 16 colorings per step
+    "tree12_rmat20_ef8": dict(scale=20, ef=8, template="tree12", per_step=16, seed=7),
+    "p3_rmat16_ef16": dict(scale=16, ef=16, template="p3", per_step=1, seed=7),
+    "tree5_rmat20_ef6": dict(scale=20, ef=6, template="tree5", per_step=10, seed=7),
+    "spider7_rmat21_ef8": dict(scale=21, ef=8, template="spider7", per_step=64, seed=7),
+}
+DEFAULT_WORKLOAD = "tree12_rmat20_ef8"
+METRIC = "colorings/sec"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+        self.index = index
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_graph(w):
+    import subgraph_b200 as sg
+    el = sg.rmat(w["scale"], w["ef"], seed=1)
+    csc = sg.CSCGraph()
+    csc.createFromEdgeListFile(el.getNumVertices(), el.getNumEdges(), el.getSrcList(), el.getDstList())
+    return el, csc
+
+
+def reference_cpu(w, csc, n_colorings: int, threads: int, workdir: str):
+    """Runs the reference's own CLI (built from its sources) on graph.data; returns
+    (seconds per coloring, kind, note) or None."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "sc-nec-ncc.bin")
+    n, edges = TEMPLATES[w["template"]]
+    tpath = os.path.join(workdir, "template.fascia")
+    with open(tpath, "w") as f:
+        f.write(f"{n}\n{len(edges)}\n" + "".join(f"{a} {b}\n" for a, b in edges))
+    if os.path.exists(exe):
+        gpath = os.path.join(workdir, "graph.data")
+        csc.serialize(gpath)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        # argv: graph template iterations threads load_binary write_binary isPruned useSPMM
+        r = subprocess.run([exe, gpath, tpath, str(n_colorings), str(threads), "1", "0", "1", "1"],
+                           capture_output=True, text=True, env=env, cwd=workdir, timeout=1800)
+        m = re.search(r"Time for count per iter:\s*([0-9.eE+-]+)", r.stdout)
+        if r.returncode == 0 and m:
+            return float(m.group(1)), "reference", threads
+        log("reference CLI failed:", r.returncode, r.stderr[-500:])
+    # fall back to the oracle port (single thread) on one coloring
+    from oracle import oracle as O
+    P = O.Plan(n, edges)
+    colors = O.colors(w["seed"], csc.getNumVertices(), n)
+    t0 = time.perf_counter()
+    O.count_coloring(csc.getIndexCol(), csc.getIndexRow(), P, colors)
+    return time.perf_counter() - t0, "port", 1
+
+
+def run_reference_arm(args, w):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    _, csc = build_graph(w)
+    threads = os.cpu_count() or 1
+    ncol = max(1, min(args.steps, 3))
+    with tempfile.TemporaryDirectory() as tmp:
+        sec, kind, cores = reference_cpu(w, csc, ncol, threads, tmp)
+    value = 1.0 / sec
+    line = {
+        "metric": METRIC, "value": value, "unit": "colorings/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1000.0, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": config_of(args, w),
+        "cpu_baseline": {"value": value, "unit": "colorings/s", "cores": cores, "kind": kind,
+                         "sample": f"{ncol} coloring(s) of the workload, one process, {cores} threads"},
+        "e2e": {"value": value, "unit": "colorings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_of(args, w):
+    return {"workload": args.workload, "graph": f"rmat scale {w['scale']} edge factor {w['ef']} seed 1",
+            "template": w["template"], "colorings_per_step": w["per_step"], "tables": "fp32",
+            "sums": "fp64", "form": "plain" if args.batch == 0 else f"batched({args.batch})",
+            "hub_threshold": args.hub, "l2": "inputs larger than L2 (count tables of several GB per coloring)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--batch", type=int, default=0, help="colorings per persistent launch (0 = plain)")
+    ap.add_argument("--hub", type=int, default=1024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference_arm(args, w)
+        return
+
+    import numpy as np
+    import torch
+
+    import subgraph_b200 as sg
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    t_build = time.perf_counter()
+    el, csc = build_graph(w)
+    g = csc.device_graph(local)
+    n, edges = TEMPLATES[w["template"]]
+    tmpl = sg.Graph(n, edges)
+    B = w["per_step"]
+    log(f"[rank {rank}] graph V={csc.getNumVertices()} nnz={csc.getNNZ()} built in {time.perf_counter() - t_build:.1f}s")
+
+    def seeds(step):  # rank-disjoint colorings
+        return w["seed"] + (step * world + rank) * B
+
+    for s in range(args.warmup):
+        sg.count(g, tmpl, B, seeds(s), batch=args.batch, hub_threshold=args.hub)
+    barrier()
+    dev_ms, launches, fused_ms, fused_launches, fused_bytes, gather_bytes, hub_ms = 0.0, 0, 0.0, 0, 0.0, 0.0, 0.0
+    raws = []
+    with Clocks(local) as clk:
+        barrier()
+        for s in range(args.steps):
+            raw, st = sg.count(g, tmpl, B, seeds(args.warmup + s), batch=args.batch, hub_threshold=args.hub,
+                               return_stats=True, profile=True)
+            raws.append(raw)
+            dev_ms += st["device_ms"]
+            launches += st["kernel_launches"]
+            fused_ms += st["fused_ms"]
+            fused_launches += st["fused_launches"]
+            fused_bytes += st["fused_alg_bytes"]
+            gather_bytes += st["fused_gather_bytes"]
+            hub_ms += st["hub_ms"]
+        barrier()
+    clocks = clk.summary()
+    total_ms = max_over_ranks(dev_ms)
+    ms_per_step = total_ms / args.steps
+    value = world * B * args.steps / (total_ms / 1000.0)
+
+    # end to end through the public API: pinned host CSC -> device graph -> count -> raw counts
+    e2e = None
+    if not args.no_e2e:
+        col = torch.from_numpy(csc.getIndexCol()).pin_memory()
+        row = torch.from_numpy(csc.getIndexRow()).pin_memory()
+        col_np, row_np = col.numpy(), row.numpy()
+        h2d = 4 * (len(col_np) + len(row_np))
+        barrier()
+        t0 = time.perf_counter()
+        for s in range(args.steps):
+            dg = sg.DeviceGraph(col_np, row_np, local)
+            sg.count(dg, tmpl, B, seeds(args.warmup + s), batch=args.batch, hub_threshold=args.hub)
+            del dg
+        barrier()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        e2e = {"value": world * B * args.steps / e2e_s, "unit": "colorings/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": 8 * B}
+
+    # precision: FP32 tables against FP64 tables on the first two colorings of the run
+    n_chk = min(2, B)
+    r64 = sg.count(g, tmpl, n_chk, seeds(args.warmup), mode=sg.MODE_FP64, hub_threshold=args.hub)
+    err = max(abs(a - b) / abs(b) for a, b in zip(raws[0][:n_chk], r64) if b != 0) if np.any(r64) else 0.0
+    err = max_over_ranks(err)
+
+    peak, peak_kind = peaks()
+    achieved = fused_bytes / (fused_ms / 1000.0) / 1e9 if fused_ms > 0 else 0.0
+    line = {
+        "metric": METRIC, "value": value, "unit": "colorings/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic", "config": config_of(args, w),
+        "rel_err_vs_fp64": err,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "kernel": "k_fused (aggregation + eMA)",
+                     "fused_ms_per_step": fused_ms / args.steps, "fused_launches_per_step": fused_launches / args.steps,
+                     "alg_bytes_per_step": fused_bytes / args.steps,
+                     "gather_bytes_per_step": gather_bytes / args.steps, "hub_ms_per_step": hub_ms / args.steps},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        with tempfile.TemporaryDirectory() as tmp:
+            sec, kind, cores = reference_cpu(w, csc, 1, os.cpu_count() or 1, tmp)
+        line["cpu_baseline"] = {"value": 1.0 / sec, "unit": "colorings/s", "cores": cores, "kind": kind,
+                                "sample": "1 coloring of the workload"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,178 @@
+/*
+ * sg_api.h -- C ABI of subgraph_b200, a B200 (sm_100a) implementation of
+ * dsc-nec/subgraph's color-coding tree-template counting engine.
+ *
+ * Conventions
+ *   - Every call returns sg_status (SG_OK = 0); sg_last_error() gives the
+ *     message of the last failure on the calling thread.  No exception crosses
+ *     the ABI.
+ *   - Pointers in the signatures are HOST pointers.  Arrays returned by the
+ *     library (sg_edgelist_read, ...) are malloc'd and released with sg_free.
+ *   - Device memory is owned by the library (per sg_graph).  A graph handle is
+ *     used by one host thread at a time.
+ *   - Vertex ids, offsets and neighbour counts are int32 like the reference's
+ *     idxType (CountMat.hpp:24); nnz <= 2^31-1.
+ *
+ * Each declaration names the reference interface it replaces (file:line in
+ * the dsc-nec/subgraph tree).
+ */
+#ifndef SG_API_H
+#define SG_API_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t sg_status;
+#define SG_OK 0
+#define SG_ERR_INVALID 1      /* bad argument, malformed input file */
+#define SG_ERR_OOM 2          /* device or host allocation failed / over budget */
+#define SG_ERR_CUDA 3         /* CUDA runtime error */
+#define SG_ERR_TIMEOUT 4      /* a bounded device wait gave up */
+#define SG_ERR_IO 5           /* file could not be read or written */
+#define SG_ERR_UNSUPPORTED 6  /* shape or option not supported */
+
+typedef struct sg_graph_s *sg_graph;   /* device-resident adjacency */
+typedef struct sg_plan_s *sg_plan;     /* template + sub-templates + index tables */
+typedef struct sg_countmat_s *sg_countmat;
+
+/* count modes */
+#define SG_MODE_REFERENCE 0   /* FP32 tables, the reference's arithmetic (isPruned=1) */
+#define SG_MODE_FP64 1        /* FP64 tables, no scaling: high-precision oracle mode */
+#define SG_MODE_ORIGINAL 2    /* FP32, isPruned=0 arithmetic (CountMat.cpp:851-977) */
+
+const char *sg_last_error(void);
+const char *sg_version(void);
+void sg_free(void *p);
+
+/* ---- host-side inputs (no GPU needed) --------------------------------- */
+
+/* EdgeList::EdgeList(fileName) / readfromEdgeList (EdgeList.hpp:28-36,
+ * EdgeList.cpp:34-116): "V\nE\nu v\n..." with hole removal. */
+sg_status sg_edgelist_read(const char *path, int32_t *V, int64_t *E, int32_t **src, int32_t **dst);
+sg_status sg_edgelist_write(const char *path, int32_t V, int64_t E, const int32_t *src, const int32_t *dst);
+
+/* CSCGraph::createFromEdgeListFile (CSCGraph.hpp:64-65, 95-178).
+ * indexCol[V+1], indexRow[2E], degList[V] are malloc'd by the library. */
+sg_status sg_csc_build(int32_t V, int64_t E, const int32_t *src, const int32_t *dst,
+                       int32_t **indexCol, int32_t **indexRow, int32_t **degList);
+
+/* CSRGraph::createFromEdgeListFile (CSRGraph.hpp:112-113, CSRGraph.cpp:16-108):
+ * row offsets indexRow[V+1], neighbours indexCol[2E] in insertion order. */
+sg_status sg_csr_build(int32_t V, int64_t E, const int32_t *src, const int32_t *dst,
+                       int32_t **indexRow, int32_t **indexCol, int32_t **degList);
+
+/* CSCGraph::serialize / deserialize (CSCGraph.hpp:71-72, 427-463): graph.data */
+sg_status sg_graph_data_write(const char *path, int32_t V, int32_t numEdges, const int32_t *indexCol,
+                              const int32_t *indexRow, const int32_t *degList);
+sg_status sg_graph_data_read(const char *path, int32_t *V, int32_t *numEdges, int32_t **indexCol,
+                             int32_t **indexRow, int32_t **degList);
+
+/* Synthetic input: seeded R-MAT (no reference counterpart in the product; the
+ * reference's inputs come from graph500's make_graph, make_graph.h:21-35). */
+sg_status sg_rmat_generate(int32_t scale, int32_t edge_factor, double a, double b, double c, uint64_t seed,
+                           int32_t *V, int64_t *E, int32_t **src, int32_t **dst);
+
+/* ---- template planning (no GPU needed) ---------------------------------- */
+
+/* Graph::read_enlist (Graph.hpp:29) + DivideTemplates::DivideTp/sort_tps
+ * (DivideTemplates.hpp:21-23) + IndexSys::initialization (IndexSys.hpp:31). */
+sg_status sg_plan_create(int32_t n, int32_t m, const int32_t *src, const int32_t *dst, sg_plan *out);
+sg_status sg_plan_read(const char *template_path, sg_plan *out);
+void sg_plan_destroy(sg_plan p);
+/* k, number of subs, the scaled sub, arena size in units of V elements */
+sg_status sg_plan_info(sg_plan p, int32_t *k, int32_t *nsub, int32_t *scaled_sub, int64_t *arena_units);
+/* per sub: size, main, aux, parent (93620 = none, DivideTemplates.hpp:26-29),
+ * L = C(k,size), S = C(size,|main|), table pitch (DataTableColMajor.hpp:27-35) */
+sg_status sg_plan_sub(sg_plan p, int32_t s, int32_t info[7]);
+/* IndexSys tables of sub s (IndexSys.hpp:35-39): c2c[L], msplit[L*S], asplit[L*S] */
+sg_status sg_plan_tables(sg_plan p, int32_t s, int32_t *c2c, int32_t *msplit, int32_t *asplit);
+/* CountMat::automorphismNum (CountMat.hpp:110) */
+sg_status sg_plan_automorphisms(sg_plan p, int32_t *count);
+/* the edges of sub s's relabelled subtree (DivideTemplates::get_subtps) */
+sg_status sg_plan_sub_edges(sg_plan p, int32_t s, int32_t *n, int32_t *src, int32_t *dst);
+
+/* ---- device graph -------------------------------------------------------- */
+
+/* Uploads an adjacency given per vertex in summation order: a CSC
+ * (indexCol, indexRow) as CountMat uses it (CountMat.hpp:32, CountMat.cpp:
+ * 686-735) or a CSR (indexRow, indexCol) for the CSRGraph path. */
+sg_status sg_graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V, int64_t nnz,
+                          int32_t device, sg_graph *out);
+void sg_graph_destroy(sg_graph g);
+sg_status sg_graph_info(sg_graph g, int32_t *V, int64_t *nnz, int32_t *max_degree);
+
+/* ---- counting ------------------------------------------------------------- */
+
+typedef struct {
+    int32_t n_colorings;    /* iterations (CountMat::initialization itr_num) */
+    uint32_t seed_base;     /* coloring c uses srand(seed_base + c) */
+    int32_t mode;           /* SG_MODE_* */
+    int32_t batch;          /* > 0: colorings per persistent launch; 0: plain */
+    int32_t hub_threshold;  /* degree above which aggregation is chunked; 0 = never
+                               (exact reference arithmetic for every vertex) */
+    int32_t profile;        /* != 0: time every fused launch with CUDA events */
+    int32_t reserved[2];
+} sg_count_opts;
+
+typedef struct {
+    double device_ms;        /* CUDA-event time of the counting launches */
+    int64_t kernel_launches; /* kernels launched by the call */
+    int64_t table_bytes;     /* device bytes of count tables */
+    /* with profile != 0: the fused aggregation+eMA launches */
+    double fused_ms;         /* summed CUDA-event time of the fused launches */
+    int64_t fused_launches;
+    double fused_alg_bytes;  /* compulsory bytes of those launches: every input table
+                                read once, the output written once, the adjacency once */
+    double fused_gather_bytes; /* neighbour-row bytes the aggregation reads (4*nnz*L_a) */
+    double hub_ms;           /* summed time of the hub aggregation launches */
+} sg_count_stats;
+
+void sg_count_opts_default(sg_count_opts *o);
+
+/* CountMat::colorCounting per coloring (CountMat.cpp:268-322): raw colorful
+ * counts, one per coloring, into raw[n_colorings] (host). */
+sg_status sg_count(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw, sg_count_stats *stats);
+
+/* CountMat::compute's final estimate (CountMat.cpp:246-264):
+ * floor(mean(raw) / (k!/k^k * automorphisms) + 0.5). */
+sg_status sg_estimate(const double *raw, int32_t n, int32_t k, int32_t automorphisms, double *out);
+
+/* ---- parity helpers ------------------------------------------------------- */
+
+/* CountMat::colorInit on one thread (CountMat.cpp:979-991): colors[V] in
+ * original vertex order. */
+sg_status sg_colors(sg_graph g, int32_t k, uint32_t seed, int32_t *colors);
+/* the count table of sub s after one coloring (DataTableColMajor columns,
+ * column-major [L][V], original order; float or double by mode) */
+sg_status sg_debug_sub_table(sg_graph g, sg_plan p, uint32_t seed, int32_t mode, int32_t hub_threshold,
+                             int32_t s, void *out);
+/* per-vertex root values (bufLastSub, CountMat.cpp:815-831) and their sum */
+sg_status sg_debug_root(sg_graph g, sg_plan p, uint32_t seed, int32_t mode, int32_t hub_threshold,
+                        double *root, double *raw);
+
+/* ---- CountMat mirror ---------------------------------------------------- */
+
+/* CountMat::initialization (CountMat.hpp:32-33).  Exactly one of the graphs is
+ * given, as in the reference (CountMat.cpp:27-30); thd_num is accepted for
+ * interface parity (the GPU ignores it). */
+sg_status sg_countmat_create(sg_countmat *out);
+void sg_countmat_destroy(sg_countmat cm);
+sg_status sg_countmat_initialization(sg_countmat cm, sg_graph csr_graph, sg_graph csc_graph, int32_t thd_num,
+                                     int32_t itr_num, int32_t isPruned, int32_t useSPMM, int32_t vtuneStart,
+                                     int32_t calculate_automorphisms);
+/* seed base for the colorings (the reference seeds with time(0)) */
+sg_status sg_countmat_set_seed(sg_countmat cm, uint32_t seed_base);
+/* CountMat::compute (CountMat.hpp:35): prints the reference's report lines to
+ * stdout when verbose != 0 and returns the rounded estimate in *result. */
+sg_status sg_countmat_compute(sg_countmat cm, sg_plan templates, int32_t isEstimate, int32_t verbose, double *result);
+/* per-coloring raw counts of the last compute (n = itr_num) */
+sg_status sg_countmat_raw(sg_countmat cm, double *raw);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SG_API_H */

@@ -1,0 +1,648 @@
+// Host side of the device engine.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+
+#include "kernels.cuh"
+
+namespace sg {
+
+#define SG_CK(call)                                                                               \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return Status{3, std::string(#call) + ": " + cudaGetErrorString(e_)};                 \
+    } while (0)
+
+#define SG_CKS(st)                 \
+    do {                           \
+        Status s_ = (st);          \
+        if (s_.code) return s_;    \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// glibc TYPE_3 stream: window s_0..s_30 of the lag-31 recurrence after
+// srandom(seed) (its r_0..r_30 by Schrage's 16807 multiply, s = r_3..r_30,
+// r_0, r_1, r_2) and polynomial arithmetic modulo P(x) = x^31 - x^28 - 1.
+// ---------------------------------------------------------------------------
+void glibc_window(uint32_t seed, uint32_t w[31])
+{
+    if (seed == 0) seed = 1;
+    int32_t r[31];
+    int32_t word = (int32_t)seed;
+    r[0] = word;
+    for (int i = 1; i < 31; ++i) {
+        int32_t hi = word / 127773, lo = word % 127773;
+        word = 16807 * lo - 2836 * hi;
+        if (word < 0) word += 2147483647;
+        r[i] = word;
+    }
+    for (int i = 0; i < 28; ++i) w[i] = (uint32_t)r[i + 3];
+    for (int i = 0; i < 3; ++i) w[28 + i] = (uint32_t)r[i];
+}
+
+namespace {
+
+using Poly = std::vector<uint32_t>;   // 31 coefficients
+
+Poly poly_mulmod(const Poly &a, const Poly &b)
+{
+    uint32_t c[61] = {0};
+    for (int i = 0; i < 31; ++i) {
+        if (!a[i]) continue;
+        for (int j = 0; j < 31; ++j) c[i + j] += a[i] * b[j];
+    }
+    for (int d = 60; d >= 31; --d) {   // x^d = x^(d-3) + x^(d-31)
+        c[d - 3] += c[d];
+        c[d - 31] += c[d];
+        c[d] = 0;
+    }
+    return Poly(c, c + 31);
+}
+
+Poly poly_xpow(uint64_t n)
+{
+    Poly r(31, 0), base(31, 0);
+    r[0] = 1;
+    base[1] = 1;
+    while (n) {
+        if (n & 1) r = poly_mulmod(r, base);
+        base = poly_mulmod(base, base);
+        n >>= 1;
+    }
+    return r;
+}
+
+int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+// Device buffers reused across count() calls on one graph.
+struct Workspace {
+    void *arena = nullptr;
+    size_t arena_bytes = 0;
+    uint8_t *colors = nullptr;
+    size_t colors_bytes = 0;
+    double *partial = nullptr;
+    size_t partial_bytes = 0;
+    double *raw = nullptr;
+    size_t raw_bytes = 0;
+    uint32_t *windows = nullptr;
+    size_t windows_bytes = 0;
+    void *hub_partial = nullptr;
+    size_t hub_partial_bytes = 0;
+    void *hub_agg = nullptr;
+    size_t hub_agg_bytes = 0;
+    int32_t *chunk_start = nullptr;
+    size_t chunk_start_bytes = 0;
+    double *root_vertex = nullptr;
+    size_t root_vertex_bytes = 0;
+};
+
+struct DevicePlanTables {
+    std::vector<uint32_t *> split;   // per sub
+    std::vector<int16_t *> rem;      // per sub
+};
+
+struct GraphState {
+    Workspace ws;
+    std::map<uint64_t, DevicePlanTables> plans;
+};
+
+std::map<const DeviceGraph *, GraphState> g_state;
+std::mutex g_state_mu;
+
+GraphState &state_of(const DeviceGraph &g)
+{
+    std::lock_guard<std::mutex> lk(g_state_mu);
+    return g_state[&g];
+}
+
+Status grow(void **p, size_t *have, size_t need)
+{
+    if (need <= *have) return Status::ok();
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *have = 0;
+    cudaError_t e = cudaMalloc(p, need);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return Status{2, "device allocation of " + std::to_string(need) + " bytes failed: " + cudaGetErrorString(e)};
+    }
+    *have = need;
+    return Status::ok();
+}
+template <typename T> Status growT(T **p, size_t *have, size_t need) { return grow((void **)p, have, need); }
+
+Status upload_plan(DeviceGraph &g, const Plan &p, DevicePlanTables &out)
+{
+    out.split.assign(p.nsub(), nullptr);
+    out.rem.assign(p.nsub(), nullptr);
+    for (int s = 0; s < p.nsub(); ++s) {
+        const SubTemplate &st = p.subs[s];
+        if (st.size <= 1) continue;
+        std::vector<uint32_t> sp((size_t)st.L * st.S);
+        for (int i = 0; i < st.L; ++i) {
+            int o = st.comb_to_count[i];
+            for (int j = 0; j < st.S; ++j)
+                sp[(size_t)o * st.S + j] = (uint32_t)st.main_split[(size_t)i * st.S + j] |
+                                           ((uint32_t)st.aux_split[(size_t)i * st.S + j] << 16);
+        }
+        SG_CK(cudaMalloc(&out.split[s], sp.size() * 4));
+        SG_CK(cudaMemcpyAsync(out.split[s], sp.data(), sp.size() * 4, cudaMemcpyHostToDevice, g.stream));
+        if (p.subs[st.main].size == 1) {
+            std::vector<int16_t> rem((size_t)st.L * p.k, -1);
+            for (int i = 0; i < st.L; ++i) {
+                int o = st.comb_to_count[i];
+                for (int j = 0; j < st.S; ++j)
+                    rem[(size_t)o * p.k + st.main_split[(size_t)i * st.S + j]] = (int16_t)st.aux_split[(size_t)i * st.S + j];
+            }
+            SG_CK(cudaMalloc(&out.rem[s], rem.size() * 2));
+            SG_CK(cudaMemcpyAsync(out.rem[s], rem.data(), rem.size() * 2, cudaMemcpyHostToDevice, g.stream));
+        }
+    }
+    SG_CK(cudaStreamSynchronize(g.stream));
+    return Status::ok();
+}
+
+struct Hubs {
+    int32_t count = 0, chunk = 0, total_chunks = 0;
+};
+
+Hubs plan_hubs(const DeviceGraph &g, int thr)
+{
+    Hubs h;
+    if (thr <= 0) return h;
+    while (h.count < g.V && g.h_degree[h.count] > thr) {
+        h.total_chunks += (g.h_degree[h.count] + thr - 1) / thr;
+        ++h.count;
+    }
+    h.chunk = thr;
+    return h;
+}
+
+}  // namespace
+
+DeviceGraph::~DeviceGraph()
+{
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    {
+        std::lock_guard<std::mutex> lk(g_state_mu);
+        auto it = g_state.find(this);
+        if (it != g_state.end()) {
+            Workspace &w = it->second.ws;
+            for (void *p : {w.arena, (void *)w.colors, (void *)w.partial, (void *)w.raw, (void *)w.windows, w.hub_partial,
+                            w.hub_agg, (void *)w.chunk_start, (void *)w.root_vertex})
+                if (p) cudaFree(p);
+            for (auto &kv : it->second.plans) {
+                for (auto *p : kv.second.split) if (p) cudaFree(p);
+                for (auto *p : kv.second.rem) if (p) cudaFree(p);
+            }
+            g_state.erase(it);
+        }
+    }
+    for (void *p : {(void *)d_off, (void *)d_adj, (void *)d_perm, (void *)d_iperm, (void *)d_jump, (void *)d_coef})
+        if (p) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+    cudaSetDevice(prev);
+}
+
+Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V, int64_t nnz, int device,
+                    std::unique_ptr<DeviceGraph> &out)
+{
+    if (V < 0 || nnz < 0 || nnz > 0x7fffffffLL) return Status{1, "vertex or entry count out of range"};
+    if (!offsets || (nnz > 0 && !neighbors)) return Status{1, "null graph array"};
+    if (offsets[0] != 0 || offsets[V] != nnz) return Status{1, "offsets[0] must be 0 and offsets[V] must equal nnz"};
+    for (int32_t v = 0; v < V; ++v)
+        if (offsets[v + 1] < offsets[v]) return Status{1, "offsets are not monotone"};
+    int ndev = 0;
+    SG_CK(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return Status{1, "no CUDA device " + std::to_string(device)};
+    SG_CK(cudaSetDevice(device));
+    auto g = std::make_unique<DeviceGraph>();
+    g->device = device;
+    g->V = V;
+    g->nnz = nnz;
+    SG_CK(cudaDeviceGetAttribute(&g->sm_count, cudaDevAttrMultiProcessorCount, device));
+    SG_CK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    // degree order: counting sort by degree, descending, stable in the id
+    std::vector<int32_t> deg(V);
+    int32_t maxd = 0;
+    for (int32_t v = 0; v < V; ++v) { deg[v] = offsets[v + 1] - offsets[v]; maxd = std::max(maxd, deg[v]); }
+    g->max_degree = maxd;
+    std::vector<int64_t> bucket((size_t)maxd + 2, 0);
+    for (int32_t v = 0; v < V; ++v) bucket[(size_t)(maxd - deg[v]) + 1]++;
+    for (size_t i = 1; i < bucket.size(); ++i) bucket[i] += bucket[i - 1];
+    std::vector<int32_t> iperm(V), perm(V), noff((size_t)V + 1);
+    for (int32_t v = 0; v < V; ++v) iperm[bucket[(size_t)(maxd - deg[v])]++] = v;
+    g->h_degree.resize(V);
+    noff[0] = 0;
+    for (int32_t i = 0; i < V; ++i) {
+        perm[iperm[i]] = i;
+        g->h_degree[i] = deg[iperm[i]];
+        noff[i + 1] = noff[i] + g->h_degree[i];
+    }
+    SG_CK(cudaMalloc(&g->d_off, sizeof(int32_t) * ((size_t)V + 1)));
+    SG_CK(cudaMalloc(&g->d_adj, sizeof(int32_t) * std::max<int64_t>(nnz, 1)));
+    SG_CK(cudaMalloc(&g->d_perm, sizeof(int32_t) * std::max<int32_t>(V, 1)));
+    SG_CK(cudaMalloc(&g->d_iperm, sizeof(int32_t) * std::max<int32_t>(V, 1)));
+    int32_t *d_old_off = nullptr, *d_old_adj = nullptr;
+    SG_CK(cudaMalloc(&d_old_off, sizeof(int32_t) * ((size_t)V + 1)));
+    SG_CK(cudaMalloc(&d_old_adj, sizeof(int32_t) * std::max<int64_t>(nnz, 1)));
+    cudaStream_t st = g->stream;
+    SG_CK(cudaMemcpyAsync(d_old_off, offsets, sizeof(int32_t) * ((size_t)V + 1), cudaMemcpyHostToDevice, st));
+    if (nnz) SG_CK(cudaMemcpyAsync(d_old_adj, neighbors, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
+    SG_CK(cudaMemcpyAsync(g->d_off, noff.data(), sizeof(int32_t) * ((size_t)V + 1), cudaMemcpyHostToDevice, st));
+    if (V) {
+        SG_CK(cudaMemcpyAsync(g->d_perm, perm.data(), sizeof(int32_t) * V, cudaMemcpyHostToDevice, st));
+        SG_CK(cudaMemcpyAsync(g->d_iperm, iperm.data(), sizeof(int32_t) * V, cudaMemcpyHostToDevice, st));
+    }
+    // neighbour ids are range-checked on the host before the remap reads them
+    for (int64_t e = 0; e < nnz; ++e)
+        if ((uint32_t)neighbors[e] >= (uint32_t)V) {
+            cudaStreamSynchronize(st);
+            cudaFree(d_old_off);
+            cudaFree(d_old_adj);
+            return Status{1, "neighbour id out of range at entry " + std::to_string(e)};
+        }
+    launch_remap(V, d_old_off, d_old_adj, g->d_off, g->d_iperm, g->d_perm, g->d_adj, st);
+    SG_CK(cudaGetLastError());
+    // coloring jump-ahead tables
+    g->color_blocks = (V + kColorBlock - 1) / kColorBlock;
+    std::vector<uint32_t> jump((size_t)std::max(g->color_blocks, 1) * 31), coef((size_t)31 * kColorBlock);
+    Poly J = poly_xpow(341), step = poly_xpow(kColorBlock);
+    for (int b = 0; b < g->color_blocks; ++b) {
+        std::copy(J.begin(), J.end(), jump.begin() + (size_t)b * 31);
+        J = poly_mulmod(J, step);
+    }
+    Poly q(31, 0);
+    q[0] = 1;
+    for (int t = 0; t < kColorBlock; ++t) {
+        for (int i = 0; i < 31; ++i) coef[(size_t)i * kColorBlock + t] = q[i];
+        uint32_t top = q[30];
+        for (int j = 30; j > 0; --j) q[j] = q[j - 1];
+        q[0] = top;
+        q[28] += top;
+    }
+    SG_CK(cudaMalloc(&g->d_jump, jump.size() * 4));
+    SG_CK(cudaMalloc(&g->d_coef, coef.size() * 4));
+    SG_CK(cudaMemcpyAsync(g->d_jump, jump.data(), jump.size() * 4, cudaMemcpyHostToDevice, st));
+    SG_CK(cudaMemcpyAsync(g->d_coef, coef.data(), coef.size() * 4, cudaMemcpyHostToDevice, st));
+    SG_CK(cudaStreamSynchronize(st));
+    cudaFree(d_old_off);
+    cudaFree(d_old_adj);
+    out = std::move(g);
+    return Status::ok();
+}
+
+namespace {
+
+struct RunCtx {
+    DeviceGraph &g;
+    const Plan &p;
+    GraphState &gs;
+    DevicePlanTables *tab;
+    bool fp64;
+    size_t es;
+    size_t arena_per_coloring;
+    Hubs hubs;
+    int32_t hub_pitch;
+    int64_t launches = 0;
+    int mode;
+    int root_tiles = 0;
+    // profiling: event pairs around every hub and fused launch
+    bool profile = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> fused_ev, hub_ev;
+    double fused_alg_bytes = 0, fused_gather_bytes = 0;
+};
+
+Status ev_pair(std::vector<std::pair<cudaEvent_t, cudaEvent_t>> &v)
+{
+    cudaEvent_t a, b;
+    SG_CK(cudaEventCreate(&a));
+    SG_CK(cudaEventCreate(&b));
+    v.push_back({a, b});
+    return Status::ok();
+}
+
+double ev_sum(std::vector<std::pair<cudaEvent_t, cudaEvent_t>> &v)
+{
+    double t = 0;
+    for (auto &e : v) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e.first, e.second);
+        t += ms;
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    v.clear();
+    return t;
+}
+
+Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
+{
+    DeviceGraph &g = c.g;
+    GraphState &gs = c.gs;
+    Workspace &w = gs.ws;
+    const size_t V = (size_t)g.V;
+    c.arena_per_coloring = (size_t)c.p.arena_units * V * c.es;
+    SG_CKS(grow(&w.arena, &w.arena_bytes, std::max<size_t>(16, c.arena_per_coloring * ncolor_slots)));
+    SG_CKS(growT(&w.colors, &w.colors_bytes, std::max<size_t>(16, V * ncolor_slots)));
+    SG_CKS(growT(&w.partial, &w.partial_bytes, 8 * ((V / 8 + 2) * ncolor_slots)));
+    SG_CKS(growT(&w.raw, &w.raw_bytes, 8 * (size_t)std::max(ncolorings_total, 1)));
+    SG_CKS(growT(&w.windows, &w.windows_bytes, 4 * 31 * (size_t)std::max(ncolorings_total, 1)));
+    if (c.hubs.count > 0) {
+        int32_t maxp = round_up(c.p.k, 4);
+        for (int s : c.p.process_order) {
+            const SubTemplate &st = c.p.subs[s];
+            const SubTemplate &a = c.p.subs[st.aux];
+            if (a.size > 1) maxp = std::max<int32_t>(maxp, c.p.table_pitch[st.aux]);
+        }
+        c.hub_pitch = maxp;
+        SG_CKS(grow(&w.hub_partial, &w.hub_partial_bytes, (size_t)c.hubs.total_chunks * maxp * c.es));
+        SG_CKS(grow(&w.hub_agg, &w.hub_agg_bytes, (size_t)c.hubs.count * maxp * c.es));
+        std::vector<int32_t> cs((size_t)c.hubs.count + 1, 0);
+        for (int h = 0; h < c.hubs.count; ++h) cs[h + 1] = cs[h] + (g.h_degree[h] + c.hubs.chunk - 1) / c.hubs.chunk;
+        SG_CKS(growT(&w.chunk_start, &w.chunk_start_bytes, 4 * cs.size()));
+        SG_CK(cudaMemcpyAsync(w.chunk_start, cs.data(), 4 * cs.size(), cudaMemcpyHostToDevice, g.stream));
+    }
+    return Status::ok();
+}
+
+void *table_ptr(RunCtx &c, int slot, int sub)
+{
+    return (char *)c.gs.ws.arena + c.arena_per_coloring * slot + (size_t)c.p.table_offset[sub] * c.g.V * c.es;
+}
+
+// One sub-template step of the coloring in color slot `slot`.
+Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t st)
+{
+    const Plan &p = c.p;
+    const SubTemplate &sub = p.subs[s];
+    const SubTemplate &m = p.subs[sub.main], &a = p.subs[sub.aux];
+    DeviceGraph &g = c.g;
+    Workspace &w = c.gs.ws;
+    StageDesc d{};
+    d.V = g.V;
+    d.L_s = sub.L;
+    d.S = sub.S;
+    d.k = p.k;
+    d.main_leaf = m.size == 1;
+    d.aux_leaf = a.size == 1;
+    d.L_m = m.L;
+    d.L_a = a.L;
+    d.is_root = s == 0;
+    d.scaled = (c.mode == kModeReference && s == p.scaled_sub && s != 0) ? 1 : 0;
+    d.root_float = c.mode == kModeOriginal;
+    d.out_pitch = s == 0 ? 0 : p.table_pitch[s];
+    d.main_pitch = d.main_leaf ? 0 : p.table_pitch[sub.main];
+    d.aux_pitch = d.aux_leaf ? 0 : p.table_pitch[sub.aux];
+    d.main = d.main_leaf ? nullptr : table_ptr(c, slot, sub.main);
+    d.aux = d.aux_leaf ? nullptr : table_ptr(c, slot, sub.aux);
+    d.out = s == 0 ? nullptr : table_ptr(c, slot, s);
+    d.split = c.tab->split[s];
+    d.rem = c.tab->rem[s];
+    d.color = w.colors + (size_t)slot * g.V;
+    d.off = g.d_off;
+    d.adj = g.d_adj;
+    d.root_partial = w.partial + (size_t)slot * (g.V / 8 + 2);
+    d.root_vertex = root_vertex;
+    if (c.hubs.count > 0) {
+        HubArgs h{};
+        h.hub_count = c.hubs.count;
+        h.chunk = c.hubs.chunk;
+        h.L_a = a.L;
+        h.aux_pitch = d.aux_pitch;
+        h.row_pitch = c.hub_pitch;
+        h.k_leaf = d.aux_leaf ? p.k : 0;
+        h.color = d.color;
+        h.total_chunks = c.hubs.total_chunks;
+        h.chunk_start = w.chunk_start;
+        h.off = g.d_off;
+        h.adj = g.d_adj;
+        h.aux = d.aux;
+        h.partial = w.hub_partial;
+        h.hub_agg = w.hub_agg;
+        if (c.profile) {
+            SG_CKS(ev_pair(c.hub_ev));
+            SG_CK(cudaEventRecord(c.hub_ev.back().first, st));
+        }
+        launch_hub(h, c.fp64, g.sm_count, st);
+        if (c.profile) SG_CK(cudaEventRecord(c.hub_ev.back().second, st));
+        c.launches += 2;
+        d.hub_count = c.hubs.count;
+        d.hub_pitch = c.hub_pitch;
+        d.hub_agg = w.hub_agg;
+    }
+    FusedConfig cfg;
+    if (!plan_fused(d, c.fp64, g.sm_count, cfg))
+        return Status{6, "sub-template " + std::to_string(s) + " needs more shared memory than a CTA has"};
+    if (c.profile) {
+        SG_CKS(ev_pair(c.fused_ev));
+        SG_CK(cudaEventRecord(c.fused_ev.back().first, st));
+    }
+    launch_fused(d, c.fp64, cfg, st);
+    if (c.profile) {
+        SG_CK(cudaEventRecord(c.fused_ev.back().second, st));
+        // compulsory traffic: main and aux tables read once (a one-hot child is read
+        // as the colors array: one element per vertex), the output written once and
+        // the adjacency read once (offsets + neighbour ids)
+        const double V = (double)g.V;
+        const double lm = d.main_leaf ? 1.0 : (double)d.L_m, la = d.aux_leaf ? 1.0 : (double)d.L_a;
+        c.fused_alg_bytes += (double)c.es * V * (lm + la + (s ? (double)d.L_s : 0.0)) + 4.0 * (V + 1 + (double)g.nnz);
+        c.fused_gather_bytes += (double)c.es * (double)g.nnz * (d.aux_leaf ? 0.25 : (double)d.L_a);
+    }
+    c.launches += 1;
+    if (s == 0) c.root_tiles = d.ntiles;
+    SG_CK(cudaGetLastError());
+    return Status::ok();
+}
+
+Status launch_colors(RunCtx &c, int slot0, int first_coloring, int n, cudaStream_t st)
+{
+    ColorArgs a{};
+    a.V = c.g.V;
+    a.k = c.p.k;
+    a.nblocks = c.g.color_blocks;
+    a.jump = c.g.d_jump;
+    a.coef = c.g.d_coef;
+    a.window = c.gs.ws.windows + 31 * (size_t)first_coloring;
+    a.perm = c.g.d_perm;
+    a.color = c.gs.ws.colors + (size_t)slot0 * c.g.V;
+    a.color_stride = c.g.V;
+    launch_color(a, n, st);
+    c.launches += 1;
+    SG_CK(cudaGetLastError());
+    return Status::ok();
+}
+
+Status make_ctx_tables(DeviceGraph &g, const Plan &p, GraphState &gs, DevicePlanTables *&tab)
+{
+    auto it = gs.plans.find(p.uid);
+    if (it == gs.plans.end()) {
+        DevicePlanTables t;
+        SG_CKS(upload_plan(g, p, t));
+        it = gs.plans.emplace(p.uid, std::move(t)).first;
+    }
+    tab = &it->second;
+    return Status::ok();
+}
+
+Status upload_windows(RunCtx &c, uint32_t seed_base, int n)
+{
+    std::vector<uint32_t> win((size_t)n * 31);
+    for (int i = 0; i < n; ++i) glibc_window(seed_base + (uint32_t)i, &win[(size_t)i * 31]);
+    SG_CK(cudaMemcpyAsync(c.gs.ws.windows, win.data(), win.size() * 4, cudaMemcpyHostToDevice, c.g.stream));
+    SG_CK(cudaStreamSynchronize(c.g.stream));   // `win` is pageable and goes out of scope
+    return Status::ok();
+}
+
+}  // namespace
+
+Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, CountStats *stats)
+{
+    if (o.n_colorings < 1) return Status{1, "n_colorings must be >= 1"};
+    if (o.mode < 0 || o.mode > 2) return Status{1, "unknown count mode"};
+    if (p.k > 255) return Status{1, "too many colors"};
+    SG_CK(cudaSetDevice(g.device));
+    GraphState &gs = state_of(g);
+    RunCtx c{g, p, gs, nullptr, o.mode == kModeFP64, (size_t)(o.mode == kModeFP64 ? 8 : 4), 0, {}, 0, 0, o.mode, 0};
+    SG_CKS(make_ctx_tables(g, p, gs, c.tab));
+    c.hubs = plan_hubs(g, o.hub_threshold);
+    c.profile = o.profile != 0;
+    const int slots = 1;
+    SG_CKS(prepare(c, slots, o.n_colorings));
+    SG_CKS(upload_windows(c, o.seed_base, o.n_colorings));
+    cudaStream_t st = g.stream;
+    cudaEvent_t e0, e1;
+    SG_CK(cudaEventCreate(&e0));
+    SG_CK(cudaEventCreate(&e1));
+    SG_CK(cudaEventRecord(e0, st));
+    const double scale = o.mode == kModeOriginal ? 1.0 : (o.mode == kModeReference ? 1.0e12 : 1.0);
+    for (int col = 0; col < o.n_colorings; ++col) {
+        SG_CKS(launch_colors(c, 0, col, 1, st));
+        for (int s : p.process_order) SG_CKS(run_stage(c, 0, s, nullptr, st));
+        launch_root_reduce(gs.ws.partial, c.root_tiles, scale, gs.ws.raw + col, st);
+        c.launches += 1;
+        SG_CK(cudaGetLastError());
+    }
+    SG_CK(cudaEventRecord(e1, st));
+    SG_CK(cudaMemcpyAsync(raw, gs.ws.raw, sizeof(double) * o.n_colorings, cudaMemcpyDeviceToHost, st));
+    SG_CK(cudaStreamSynchronize(st));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (stats) {
+        stats->device_ms = ms;
+        stats->kernel_launches = c.launches;
+        stats->table_bytes = (int64_t)(c.arena_per_coloring * slots);
+        stats->fused_launches = (int64_t)c.fused_ev.size();
+        stats->fused_ms = ev_sum(c.fused_ev);
+        stats->hub_ms = ev_sum(c.hub_ev);
+        stats->fused_alg_bytes = c.fused_alg_bytes;
+        stats->fused_gather_bytes = c.fused_gather_bytes;
+    }
+    ev_sum(c.fused_ev);
+    ev_sum(c.hub_ev);
+    return Status::ok();
+}
+
+Status debug_colors(DeviceGraph &g, int k, uint32_t seed, int32_t *colors)
+{
+    if (k < 1 || k > 255) return Status{1, "k out of range"};
+    SG_CK(cudaSetDevice(g.device));
+    GraphState &gs = state_of(g);
+    Plan dummy;
+    dummy.k = k;
+    RunCtx c{g, dummy, gs, nullptr, false, 4, 0, {}, 0, 0, 0, 0};
+    SG_CKS(growT(&gs.ws.colors, &gs.ws.colors_bytes, std::max<size_t>(16, (size_t)g.V)));
+    SG_CKS(growT(&gs.ws.windows, &gs.ws.windows_bytes, 4 * 31));
+    SG_CKS(upload_windows(c, seed, 1));
+    SG_CKS(launch_colors(c, 0, 0, 1, g.stream));
+    std::vector<uint8_t> ci(g.V);
+    std::vector<int32_t> perm(g.V);
+    if (g.V) {
+        SG_CK(cudaMemcpyAsync(ci.data(), gs.ws.colors, g.V, cudaMemcpyDeviceToHost, g.stream));
+        SG_CK(cudaMemcpyAsync(perm.data(), g.d_perm, 4 * (size_t)g.V, cudaMemcpyDeviceToHost, g.stream));
+    }
+    SG_CK(cudaStreamSynchronize(g.stream));
+    for (int32_t v = 0; v < g.V; ++v) colors[v] = ci[perm[v]];
+    return Status::ok();
+}
+
+static Status run_partial(DeviceGraph &g, const Plan &p, uint32_t seed, int mode, int hub_threshold, int upto,
+                          RunCtx &c, GraphState &gs)
+{
+    SG_CKS(make_ctx_tables(g, p, gs, c.tab));
+    c.hubs = plan_hubs(g, hub_threshold);
+    SG_CKS(prepare(c, 1, 1));
+    SG_CKS(upload_windows(c, seed, 1));
+    SG_CKS(launch_colors(c, 0, 0, 1, g.stream));
+    for (int s : p.process_order) {
+        if (s < upto) break;
+        SG_CKS(run_stage(c, 0, s, upto == 0 ? gs.ws.root_vertex : nullptr, g.stream));
+    }
+    SG_CK(cudaStreamSynchronize(g.stream));
+    return Status::ok();
+}
+
+Status debug_sub_table(DeviceGraph &g, const Plan &p, uint32_t seed, int mode, int hub_threshold, int s, void *out)
+{
+    if (s <= 0 || s >= p.nsub()) return Status{1, "sub index must be in [1, nsub)"};
+    SG_CK(cudaSetDevice(g.device));
+    GraphState &gs = state_of(g);
+    RunCtx c{g, p, gs, nullptr, mode == kModeFP64, (size_t)(mode == kModeFP64 ? 8 : 4), 0, {}, 0, 0, mode, 0};
+    const SubTemplate &sub = p.subs[s];
+    std::vector<int32_t> perm(g.V);
+    if (g.V) SG_CK(cudaMemcpy(perm.data(), g.d_perm, 4 * (size_t)g.V, cudaMemcpyDeviceToHost));
+    const size_t V = (size_t)g.V;
+    if (sub.size == 1) {
+        std::vector<int32_t> col(V);
+        SG_CKS(debug_colors(g, p.k, seed, col.data()));
+        for (int cc = 0; cc < sub.L; ++cc)
+            for (size_t v = 0; v < V; ++v) {
+                double val = col[v] == cc ? 1.0 : 0.0;
+                if (c.fp64) ((double *)out)[cc * V + v] = val;
+                else ((float *)out)[cc * V + v] = (float)val;
+            }
+        return Status::ok();
+    }
+    SG_CKS(run_partial(g, p, seed, mode, hub_threshold, s, c, gs));
+    const int P = p.table_pitch[s];
+    std::vector<char> rows(V * P * c.es);
+    if (V) SG_CK(cudaMemcpy(rows.data(), table_ptr(c, 0, s), rows.size(), cudaMemcpyDeviceToHost));
+    for (size_t v = 0; v < V; ++v)
+        for (int cc = 0; cc < sub.L; ++cc) {
+            size_t src = ((size_t)perm[v] * P + cc) * c.es, dst = ((size_t)cc * V + v) * c.es;
+            std::memcpy((char *)out + dst, rows.data() + src, c.es);
+        }
+    return Status::ok();
+}
+
+Status debug_root(DeviceGraph &g, const Plan &p, uint32_t seed, int mode, int hub_threshold, double *root, double *raw)
+{
+    SG_CK(cudaSetDevice(g.device));
+    GraphState &gs = state_of(g);
+    RunCtx c{g, p, gs, nullptr, mode == kModeFP64, (size_t)(mode == kModeFP64 ? 8 : 4), 0, {}, 0, 0, mode, 0};
+    SG_CKS(growT(&gs.ws.root_vertex, &gs.ws.root_vertex_bytes, 8 * std::max<size_t>(1, (size_t)g.V)));
+    SG_CKS(run_partial(g, p, seed, mode, hub_threshold, 0, c, gs));
+    std::vector<double> rv(g.V);
+    std::vector<int32_t> perm(g.V);
+    if (g.V) {
+        SG_CK(cudaMemcpy(rv.data(), gs.ws.root_vertex, 8 * (size_t)g.V, cudaMemcpyDeviceToHost));
+        SG_CK(cudaMemcpy(perm.data(), g.d_perm, 4 * (size_t)g.V, cudaMemcpyDeviceToHost));
+    }
+    for (int32_t v = 0; v < g.V; ++v) root[v] = rv[perm[v]];
+    if (raw) {
+        double s = 0;
+        for (int32_t v = 0; v < g.V; ++v) s += root[v];
+        *raw = mode == kModeReference ? s * 1.0e12 : s;
+    }
+    return Status::ok();
+}
+
+}  // namespace sg

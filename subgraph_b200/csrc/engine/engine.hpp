@@ -1,0 +1,82 @@
+// Host side of the device engine: device-resident graphs, plans and the
+// counting pipelines (plain: launches per coloring and sub; batched: one
+// persistent work-queue launch for many colorings).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../host/plan.hpp"
+#include "stage.cuh"
+
+namespace sg {
+
+struct Status {
+    int code = 0;       // 0 ok; see include/sg_api.h for the codes
+    std::string msg;
+    static Status ok() { return {}; }
+};
+
+// A graph resident on one GPU.  Vertices are relabelled by descending degree
+// (ties by id) so that tiles of consecutive vertices have similar work and the
+// highest-degree rows share cache lines; each neighbour list keeps the order
+// of the input adjacency, which fixes the floating-point summation order.
+struct DeviceGraph {
+    int device = 0;
+    int32_t V = 0;
+    int64_t nnz = 0;
+    int32_t max_degree = 0;
+    int32_t *d_off = nullptr;     // [V+1] internal order
+    int32_t *d_adj = nullptr;     // [nnz]
+    int32_t *d_perm = nullptr;    // original -> internal
+    int32_t *d_iperm = nullptr;   // internal -> original
+    std::vector<int32_t> h_degree;   // internal order (descending)
+    // coloring jump-ahead tables
+    int32_t color_blocks = 0;
+    uint32_t *d_jump = nullptr;   // [color_blocks][31]
+    uint32_t *d_coef = nullptr;   // [31][1024]
+    cudaStream_t stream = nullptr;
+    int sm_count = 148;
+    ~DeviceGraph();
+};
+
+struct CountOptions {
+    int32_t n_colorings = 1;
+    uint32_t seed_base = 0;
+    int32_t mode = kModeReference;
+    int32_t batch = 0;              // > 0: colorings per persistent launch; 0: plain
+    int32_t hub_threshold = 1024;   // degree above which a vertex is aggregated in chunks; 0 = never
+    int32_t profile = 0;            // time every fused launch with CUDA events
+};
+
+struct CountStats {
+    double device_ms = 0;       // CUDA-event time of the counting launches
+    int64_t kernel_launches = 0;
+    int64_t table_bytes = 0;    // device bytes of count tables
+    double fused_ms = 0;        // profile: summed time of the fused launches
+    int64_t fused_launches = 0;
+    double fused_alg_bytes = 0; // compulsory bytes of the fused launches
+    double fused_gather_bytes = 0;
+    double hub_ms = 0;
+};
+
+Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V, int64_t nnz, int device,
+                    std::unique_ptr<DeviceGraph> &out);
+
+// Runs n_colorings colorings, writes the raw colorful counts (host).
+Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, CountStats *stats);
+
+// Parity helpers: colors of one seed (original order), the table of sub s
+// after one coloring (column-major [L][V], original order), per-vertex root.
+Status debug_colors(DeviceGraph &g, int k, uint32_t seed, int32_t *colors);
+Status debug_sub_table(DeviceGraph &g, const Plan &p, uint32_t seed, int mode, int hub_threshold, int s, void *out);
+Status debug_root(DeviceGraph &g, const Plan &p, uint32_t seed, int mode, int hub_threshold, double *root, double *raw);
+
+// host-side coloring tables (also used by tests through the C ABI)
+void glibc_window(uint32_t seed, uint32_t w[31]);
+
+}  // namespace sg
