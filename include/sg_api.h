@@ -114,7 +114,13 @@ typedef struct {
     int32_t hub_threshold;  /* degree above which aggregation is chunked; 0 = never
                                (exact reference arithmetic for every vertex) */
     int32_t profile;        /* != 0: time every fused launch with CUDA events */
-    int32_t reserved[2];
+    int32_t no_autotune;    /* != 0: use the default tile shapes instead of timing the
+                               candidates of each new stage shape once per graph */
+    int32_t exact;          /* != 0: the reference's FP32 operations in the reference's
+                               order for every vertex and product (no hub chunking, no
+                               fused multiply-add): per-vertex values bit-identical to
+                               the reference; otherwise products may be fused (one
+                               rounding) and hub neighbour lists summed in chunks */
 } sg_count_opts;
 
 typedef struct {

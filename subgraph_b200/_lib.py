@@ -47,7 +47,7 @@ class SGError(RuntimeError):
 class CountOpts(ctypes.Structure):
     _fields_ = [("n_colorings", ctypes.c_int32), ("seed_base", ctypes.c_uint32), ("mode", ctypes.c_int32),
                 ("batch", ctypes.c_int32), ("hub_threshold", ctypes.c_int32), ("profile", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 2)]
+                ("no_autotune", ctypes.c_int32), ("exact", ctypes.c_int32)]
 
 
 class CountStats(ctypes.Structure):

@@ -309,6 +309,8 @@ sg_status sg_count(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw, s
     co.batch = o->batch;
     co.hub_threshold = o->hub_threshold;
     co.profile = o->profile;
+    co.autotune = o->no_autotune ? 0 : 1;
+    co.exact = o->exact ? 1 : 0;
     sg::CountStats cs;
     sg_status st = from(sg::count(*g->g, p->p, co, raw, &cs));
     if (st) return st;

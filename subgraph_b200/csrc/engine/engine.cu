@@ -2,10 +2,13 @@
 #include "engine.hpp"
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 
 #include "kernels.cuh"
+#include "tile.cuh"
 
 namespace sg {
 
@@ -91,8 +94,6 @@ struct Workspace {
     size_t windows_bytes = 0;
     void *hub_partial = nullptr;
     size_t hub_partial_bytes = 0;
-    void *hub_agg = nullptr;
-    size_t hub_agg_bytes = 0;
     int32_t *chunk_start = nullptr;
     size_t chunk_start_bytes = 0;
     double *root_vertex = nullptr;
@@ -102,12 +103,22 @@ struct Workspace {
 struct DevicePlanTables {
     std::vector<uint32_t *> split;   // per sub
     std::vector<int16_t *> rem;      // per sub
+    std::vector<uint32_t *> aoff, moff;  // per sub: packed-layout byte offsets (FP32)
 };
 
 struct GraphState {
     Workspace ws;
     std::map<uint64_t, DevicePlanTables> plans;
+    std::map<std::string, TileShape> tuned;   // stage shape -> tile shape
 };
+
+std::string shape_key(const StageDesc &d, bool fp64, int hubs)
+{
+    char b[160];
+    std::snprintf(b, sizeof b, "%d/%d/%d/%d/%d/%d/%d/%d/%d/%d", d.L_s, d.S, d.L_m, d.L_a, d.main_leaf, d.aux_leaf,
+                  d.is_root, (int)fp64, d.k, hubs);
+    return b;
+}
 
 std::map<const DeviceGraph *, GraphState> g_state;
 std::mutex g_state_mu;
@@ -118,13 +129,26 @@ GraphState &state_of(const DeviceGraph &g)
     return g_state[&g];
 }
 
-Status grow(void **p, size_t *have, size_t need)
+// Device memory comes from the stream-ordered allocator of the device's
+// default pool, which keeps freed memory (release threshold = max): the
+// buffers of a destroyed graph are reused by the next one without new
+// driver allocations.
+void keep_pool_memory(int device)
+{
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+}
+
+Status grow(void **p, size_t *have, size_t need, cudaStream_t st)
 {
     if (need <= *have) return Status::ok();
-    if (*p) cudaFree(*p);
+    if (*p) cudaFreeAsync(*p, st);
     *p = nullptr;
     *have = 0;
-    cudaError_t e = cudaMalloc(p, need);
+    cudaError_t e = cudaMallocAsync(p, need, st);
     if (e != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
@@ -133,24 +157,44 @@ Status grow(void **p, size_t *have, size_t need)
     *have = need;
     return Status::ok();
 }
-template <typename T> Status growT(T **p, size_t *have, size_t need) { return grow((void **)p, have, need); }
+template <typename T> Status growT(T **p, size_t *have, size_t need, cudaStream_t st) { return grow((void **)p, have, need, st); }
 
 Status upload_plan(DeviceGraph &g, const Plan &p, DevicePlanTables &out)
 {
     out.split.assign(p.nsub(), nullptr);
     out.rem.assign(p.nsub(), nullptr);
+    out.aoff.assign(p.nsub(), nullptr);
+    out.moff.assign(p.nsub(), nullptr);
     for (int s = 0; s < p.nsub(); ++s) {
         const SubTemplate &st = p.subs[s];
         if (st.size <= 1) continue;
-        std::vector<uint32_t> sp((size_t)st.L * st.S);
+        // [split j][output column], columns padded to a multiple of 4 (zero pairs)
+        const size_t Lsp = (size_t)(st.L + 3) / 4 * 4;
+        std::vector<uint32_t> sp(Lsp * st.S, 0u);
         for (int i = 0; i < st.L; ++i) {
             int o = st.comb_to_count[i];
             for (int j = 0; j < st.S; ++j)
-                sp[(size_t)o * st.S + j] = (uint32_t)st.main_split[(size_t)i * st.S + j] |
-                                           ((uint32_t)st.aux_split[(size_t)i * st.S + j] << 16);
+                sp[(size_t)j * Lsp + o] = (uint32_t)st.main_split[(size_t)i * st.S + j] |
+                                          ((uint32_t)st.aux_split[(size_t)i * st.S + j] << 16);
         }
-        SG_CK(cudaMalloc(&out.split[s], sp.size() * 4));
+        SG_CK(cudaMallocAsync(&out.split[s], sp.size() * 4, g.stream));
         SG_CK(cudaMemcpyAsync(out.split[s], sp.data(), sp.size() * 4, cudaMemcpyHostToDevice, g.stream));
+        if (p.subs[st.main].size > 1 && s != 0) {
+            // packed eMA: byte offsets of the aggregate row and of the main row
+            // (main rows follow the La_rows aggregate rows) in the shared tile
+            const uint32_t rowb = (uint32_t)(kPackedRow * sizeof(float));
+            const uint32_t La_rows = p.subs[st.aux].size == 1 ? (uint32_t)p.k : (uint32_t)p.subs[st.aux].L;
+            std::vector<uint32_t> ao(sp.size(), 0u), mo(sp.size(), La_rows * rowb);
+            for (size_t i = 0; i < sp.size(); ++i) {
+                ao[i] = (sp[i] >> 16) * rowb;
+                mo[i] = (La_rows + (sp[i] & 0xffffu)) * rowb;
+            }
+            SG_CK(cudaMallocAsync(&out.aoff[s], ao.size() * 4, g.stream));
+            SG_CK(cudaMallocAsync(&out.moff[s], mo.size() * 4, g.stream));
+            SG_CK(cudaMemcpyAsync(out.aoff[s], ao.data(), ao.size() * 4, cudaMemcpyHostToDevice, g.stream));
+            SG_CK(cudaMemcpyAsync(out.moff[s], mo.data(), mo.size() * 4, cudaMemcpyHostToDevice, g.stream));
+            SG_CK(cudaStreamSynchronize(g.stream));
+        }
         if (p.subs[st.main].size == 1) {
             std::vector<int16_t> rem((size_t)st.L * p.k, -1);
             for (int i = 0; i < st.L; ++i) {
@@ -158,7 +202,7 @@ Status upload_plan(DeviceGraph &g, const Plan &p, DevicePlanTables &out)
                 for (int j = 0; j < st.S; ++j)
                     rem[(size_t)o * p.k + st.main_split[(size_t)i * st.S + j]] = (int16_t)st.aux_split[(size_t)i * st.S + j];
             }
-            SG_CK(cudaMalloc(&out.rem[s], rem.size() * 2));
+            SG_CK(cudaMallocAsync(&out.rem[s], rem.size() * 2, g.stream));
             SG_CK(cudaMemcpyAsync(out.rem[s], rem.data(), rem.size() * 2, cudaMemcpyHostToDevice, g.stream));
         }
     }
@@ -195,18 +239,23 @@ DeviceGraph::~DeviceGraph()
         if (it != g_state.end()) {
             Workspace &w = it->second.ws;
             for (void *p : {w.arena, (void *)w.colors, (void *)w.partial, (void *)w.raw, (void *)w.windows, w.hub_partial,
-                            w.hub_agg, (void *)w.chunk_start, (void *)w.root_vertex})
-                if (p) cudaFree(p);
+                            (void *)w.chunk_start, (void *)w.root_vertex})
+                if (p) cudaFreeAsync(p, stream);
             for (auto &kv : it->second.plans) {
-                for (auto *p : kv.second.split) if (p) cudaFree(p);
-                for (auto *p : kv.second.rem) if (p) cudaFree(p);
+                for (auto *p : kv.second.split) if (p) cudaFreeAsync(p, stream);
+                for (auto *p : kv.second.rem) if (p) cudaFreeAsync(p, stream);
+                for (auto *p : kv.second.aoff) if (p) cudaFreeAsync(p, stream);
+                for (auto *p : kv.second.moff) if (p) cudaFreeAsync(p, stream);
             }
             g_state.erase(it);
         }
     }
     for (void *p : {(void *)d_off, (void *)d_adj, (void *)d_perm, (void *)d_iperm, (void *)d_jump, (void *)d_coef})
-        if (p) cudaFree(p);
-    if (stream) cudaStreamDestroy(stream);
+        if (p) cudaFreeAsync(p, stream);
+    if (stream) {
+        cudaStreamSynchronize(stream);
+        cudaStreamDestroy(stream);
+    }
     cudaSetDevice(prev);
 }
 
@@ -228,6 +277,7 @@ Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V,
     g->nnz = nnz;
     SG_CK(cudaDeviceGetAttribute(&g->sm_count, cudaDevAttrMultiProcessorCount, device));
     SG_CK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    keep_pool_memory(device);
     // degree order: counting sort by degree, descending, stable in the id
     std::vector<int32_t> deg(V);
     int32_t maxd = 0;
@@ -245,13 +295,13 @@ Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V,
         g->h_degree[i] = deg[iperm[i]];
         noff[i + 1] = noff[i] + g->h_degree[i];
     }
-    SG_CK(cudaMalloc(&g->d_off, sizeof(int32_t) * ((size_t)V + 1)));
-    SG_CK(cudaMalloc(&g->d_adj, sizeof(int32_t) * std::max<int64_t>(nnz, 1)));
-    SG_CK(cudaMalloc(&g->d_perm, sizeof(int32_t) * std::max<int32_t>(V, 1)));
-    SG_CK(cudaMalloc(&g->d_iperm, sizeof(int32_t) * std::max<int32_t>(V, 1)));
+    SG_CK(cudaMallocAsync(&g->d_off, sizeof(int32_t) * ((size_t)V + 1), g->stream));
+    SG_CK(cudaMallocAsync(&g->d_adj, sizeof(int32_t) * std::max<int64_t>(nnz, 1), g->stream));
+    SG_CK(cudaMallocAsync(&g->d_perm, sizeof(int32_t) * std::max<int32_t>(V, 1), g->stream));
+    SG_CK(cudaMallocAsync(&g->d_iperm, sizeof(int32_t) * std::max<int32_t>(V, 1), g->stream));
     int32_t *d_old_off = nullptr, *d_old_adj = nullptr;
-    SG_CK(cudaMalloc(&d_old_off, sizeof(int32_t) * ((size_t)V + 1)));
-    SG_CK(cudaMalloc(&d_old_adj, sizeof(int32_t) * std::max<int64_t>(nnz, 1)));
+    SG_CK(cudaMallocAsync(&d_old_off, sizeof(int32_t) * ((size_t)V + 1), g->stream));
+    SG_CK(cudaMallocAsync(&d_old_adj, sizeof(int32_t) * std::max<int64_t>(nnz, 1), g->stream));
     cudaStream_t st = g->stream;
     SG_CK(cudaMemcpyAsync(d_old_off, offsets, sizeof(int32_t) * ((size_t)V + 1), cudaMemcpyHostToDevice, st));
     if (nnz) SG_CK(cudaMemcpyAsync(d_old_adj, neighbors, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
@@ -263,9 +313,9 @@ Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V,
     // neighbour ids are range-checked on the host before the remap reads them
     for (int64_t e = 0; e < nnz; ++e)
         if ((uint32_t)neighbors[e] >= (uint32_t)V) {
+            cudaFreeAsync(d_old_off, st);
+            cudaFreeAsync(d_old_adj, st);
             cudaStreamSynchronize(st);
-            cudaFree(d_old_off);
-            cudaFree(d_old_adj);
             return Status{1, "neighbour id out of range at entry " + std::to_string(e)};
         }
     launch_remap(V, d_old_off, d_old_adj, g->d_off, g->d_iperm, g->d_perm, g->d_adj, st);
@@ -287,13 +337,13 @@ Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V,
         q[0] = top;
         q[28] += top;
     }
-    SG_CK(cudaMalloc(&g->d_jump, jump.size() * 4));
-    SG_CK(cudaMalloc(&g->d_coef, coef.size() * 4));
+    SG_CK(cudaMallocAsync(&g->d_jump, jump.size() * 4, g->stream));
+    SG_CK(cudaMallocAsync(&g->d_coef, coef.size() * 4, g->stream));
     SG_CK(cudaMemcpyAsync(g->d_jump, jump.data(), jump.size() * 4, cudaMemcpyHostToDevice, st));
     SG_CK(cudaMemcpyAsync(g->d_coef, coef.data(), coef.size() * 4, cudaMemcpyHostToDevice, st));
+    cudaFreeAsync(d_old_off, st);
+    cudaFreeAsync(d_old_adj, st);
     SG_CK(cudaStreamSynchronize(st));
-    cudaFree(d_old_off);
-    cudaFree(d_old_adj);
     out = std::move(g);
     return Status::ok();
 }
@@ -315,6 +365,8 @@ struct RunCtx {
     int root_tiles = 0;
     // profiling: event pairs around every hub and fused launch
     bool profile = false;
+    bool autotune = false;
+    bool exact = false;      // no fused products (packed eMA), no hub chunks
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> fused_ev, hub_ev;
     double fused_alg_bytes = 0, fused_gather_bytes = 0;
 };
@@ -349,11 +401,11 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
     Workspace &w = gs.ws;
     const size_t V = (size_t)g.V;
     c.arena_per_coloring = (size_t)c.p.arena_units * V * c.es;
-    SG_CKS(grow(&w.arena, &w.arena_bytes, std::max<size_t>(16, c.arena_per_coloring * ncolor_slots)));
-    SG_CKS(growT(&w.colors, &w.colors_bytes, std::max<size_t>(16, V * ncolor_slots)));
-    SG_CKS(growT(&w.partial, &w.partial_bytes, 8 * ((V / 8 + 2) * ncolor_slots)));
-    SG_CKS(growT(&w.raw, &w.raw_bytes, 8 * (size_t)std::max(ncolorings_total, 1)));
-    SG_CKS(growT(&w.windows, &w.windows_bytes, 4 * 31 * (size_t)std::max(ncolorings_total, 1)));
+    SG_CKS(grow(&w.arena, &w.arena_bytes, std::max<size_t>(16, c.arena_per_coloring * ncolor_slots), g.stream));
+    SG_CKS(growT(&w.colors, &w.colors_bytes, std::max<size_t>(16, V * ncolor_slots), g.stream));
+    SG_CKS(growT(&w.partial, &w.partial_bytes, 8 * ((V / 8 + 2) * ncolor_slots), g.stream));
+    SG_CKS(growT(&w.raw, &w.raw_bytes, 8 * (size_t)std::max(ncolorings_total, 1), g.stream));
+    SG_CKS(growT(&w.windows, &w.windows_bytes, 4 * 31 * (size_t)std::max(ncolorings_total, 1), g.stream));
     if (c.hubs.count > 0) {
         int32_t maxp = round_up(c.p.k, 4);
         for (int s : c.p.process_order) {
@@ -362,11 +414,10 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
             if (a.size > 1) maxp = std::max<int32_t>(maxp, c.p.table_pitch[st.aux]);
         }
         c.hub_pitch = maxp;
-        SG_CKS(grow(&w.hub_partial, &w.hub_partial_bytes, (size_t)c.hubs.total_chunks * maxp * c.es));
-        SG_CKS(grow(&w.hub_agg, &w.hub_agg_bytes, (size_t)c.hubs.count * maxp * c.es));
+        SG_CKS(grow(&w.hub_partial, &w.hub_partial_bytes, (size_t)c.hubs.total_chunks * maxp * c.es, g.stream));
         std::vector<int32_t> cs((size_t)c.hubs.count + 1, 0);
         for (int h = 0; h < c.hubs.count; ++h) cs[h + 1] = cs[h] + (g.h_degree[h] + c.hubs.chunk - 1) / c.hubs.chunk;
-        SG_CKS(growT(&w.chunk_start, &w.chunk_start_bytes, 4 * cs.size()));
+        SG_CKS(growT(&w.chunk_start, &w.chunk_start_bytes, 4 * cs.size(), g.stream));
         SG_CK(cudaMemcpyAsync(w.chunk_start, cs.data(), 4 * cs.size(), cudaMemcpyHostToDevice, g.stream));
     }
     return Status::ok();
@@ -404,7 +455,11 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
     d.aux = d.aux_leaf ? nullptr : table_ptr(c, slot, sub.aux);
     d.out = s == 0 ? nullptr : table_ptr(c, slot, s);
     d.split = c.tab->split[s];
+    d.split_stride = (sub.L + 3) / 4 * 4;
     d.rem = c.tab->rem[s];
+    // the packed eMA fuses multiply and add: only outside exact mode
+    d.aoff = c.exact ? nullptr : c.tab->aoff[s];
+    d.moff = c.exact ? nullptr : c.tab->moff[s];
     d.color = w.colors + (size_t)slot * g.V;
     d.off = g.d_off;
     d.adj = g.d_adj;
@@ -425,21 +480,57 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
         h.adj = g.d_adj;
         h.aux = d.aux;
         h.partial = w.hub_partial;
-        h.hub_agg = w.hub_agg;
         if (c.profile) {
             SG_CKS(ev_pair(c.hub_ev));
             SG_CK(cudaEventRecord(c.hub_ev.back().first, st));
         }
         launch_hub(h, c.fp64, g.sm_count, st);
         if (c.profile) SG_CK(cudaEventRecord(c.hub_ev.back().second, st));
-        c.launches += 2;
+        c.launches += 1;
         d.hub_count = c.hubs.count;
         d.hub_pitch = c.hub_pitch;
-        d.hub_agg = w.hub_agg;
+        d.hub_chunk_start = w.chunk_start;
+        d.hub_partial = w.hub_partial;
     }
     FusedConfig cfg;
     if (!plan_fused(d, c.fp64, g.sm_count, cfg))
         return Status{6, "sub-template " + std::to_string(s) + " needs more shared memory than a CTA has"};
+    {
+        // autotuner: the first time a stage shape runs on this graph, time every
+        // (tile vertices, CTA threads) candidate on the real inputs; all of them
+        // compute the same values, so the trial launches only cost time
+        const std::string key = shape_key(d, c.fp64, c.hubs.count) + (d.aoff ? "/pk" : "/ex");
+        auto it = c.gs.tuned.find(key);
+        if (it == c.gs.tuned.end() && c.autotune) {
+            cudaEvent_t e0, e1;
+            SG_CK(cudaEventCreate(&e0));
+            SG_CK(cudaEventCreate(&e1));
+            float best = 1e30f;
+            TileShape pick{d.tile_v, d.nthreads, d.packed};
+            for (auto cand : candidate_shapes(d, c.fp64)) {
+                StageDesc dc = d;
+                if (!set_shape(dc, c.fp64, cand)) continue;
+                FusedConfig cc = cfg;
+                cc.smem = dc.smem;
+                SG_CK(cudaEventRecord(e0, st));
+                launch_fused(dc, c.fp64, cc, st);
+                SG_CK(cudaEventRecord(e1, st));
+                SG_CK(cudaEventSynchronize(e1));
+                SG_CK(cudaGetLastError());
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                c.launches += 1;
+                if (ms < best) { best = ms; pick = cand; }
+                if (std::getenv("SG_TUNE_LOG"))
+                    std::fprintf(stderr, "[sg tune] sub %d shape %s tile %d threads %d packed %d q %d group %d: %.3f ms\n",
+                                 s, key.c_str(), cand.tile_v, cand.threads, cand.packed, dc.gather_q, dc.gather_group, ms);
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            it = c.gs.tuned.emplace(key, pick).first;
+        }
+        if (it != c.gs.tuned.end() && set_shape(d, c.fp64, it->second)) cfg.smem = d.smem;
+    }
     if (c.profile) {
         SG_CKS(ev_pair(c.fused_ev));
         SG_CK(cudaEventRecord(c.fused_ev.back().first, st));
@@ -511,8 +602,10 @@ Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, 
     GraphState &gs = state_of(g);
     RunCtx c{g, p, gs, nullptr, o.mode == kModeFP64, (size_t)(o.mode == kModeFP64 ? 8 : 4), 0, {}, 0, 0, o.mode, 0};
     SG_CKS(make_ctx_tables(g, p, gs, c.tab));
-    c.hubs = plan_hubs(g, o.hub_threshold);
+    c.exact = o.exact != 0;
+    c.hubs = plan_hubs(g, c.exact ? 0 : o.hub_threshold);
     c.profile = o.profile != 0;
+    c.autotune = o.autotune != 0;
     const int slots = 1;
     SG_CKS(prepare(c, slots, o.n_colorings));
     SG_CKS(upload_windows(c, o.seed_base, o.n_colorings));
@@ -559,8 +652,8 @@ Status debug_colors(DeviceGraph &g, int k, uint32_t seed, int32_t *colors)
     Plan dummy;
     dummy.k = k;
     RunCtx c{g, dummy, gs, nullptr, false, 4, 0, {}, 0, 0, 0, 0};
-    SG_CKS(growT(&gs.ws.colors, &gs.ws.colors_bytes, std::max<size_t>(16, (size_t)g.V)));
-    SG_CKS(growT(&gs.ws.windows, &gs.ws.windows_bytes, 4 * 31));
+    SG_CKS(growT(&gs.ws.colors, &gs.ws.colors_bytes, std::max<size_t>(16, (size_t)g.V), g.stream));
+    SG_CKS(growT(&gs.ws.windows, &gs.ws.windows_bytes, 4 * 31, g.stream));
     SG_CKS(upload_windows(c, seed, 1));
     SG_CKS(launch_colors(c, 0, 0, 1, g.stream));
     std::vector<uint8_t> ci(g.V);
@@ -578,6 +671,8 @@ static Status run_partial(DeviceGraph &g, const Plan &p, uint32_t seed, int mode
                           RunCtx &c, GraphState &gs)
 {
     SG_CKS(make_ctx_tables(g, p, gs, c.tab));
+    // the parity helpers are exact when no hub chunking is asked for
+    c.exact = hub_threshold == 0;
     c.hubs = plan_hubs(g, hub_threshold);
     SG_CKS(prepare(c, 1, 1));
     SG_CKS(upload_windows(c, seed, 1));
@@ -628,7 +723,7 @@ Status debug_root(DeviceGraph &g, const Plan &p, uint32_t seed, int mode, int hu
     SG_CK(cudaSetDevice(g.device));
     GraphState &gs = state_of(g);
     RunCtx c{g, p, gs, nullptr, mode == kModeFP64, (size_t)(mode == kModeFP64 ? 8 : 4), 0, {}, 0, 0, mode, 0};
-    SG_CKS(growT(&gs.ws.root_vertex, &gs.ws.root_vertex_bytes, 8 * std::max<size_t>(1, (size_t)g.V)));
+    SG_CKS(growT(&gs.ws.root_vertex, &gs.ws.root_vertex_bytes, 8 * std::max<size_t>(1, (size_t)g.V), g.stream));
     SG_CKS(run_partial(g, p, seed, mode, hub_threshold, 0, c, gs));
     std::vector<double> rv(g.V);
     std::vector<int32_t> perm(g.V);

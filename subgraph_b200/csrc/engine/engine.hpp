@@ -51,6 +51,8 @@ struct CountOptions {
     int32_t batch = 0;              // > 0: colorings per persistent launch; 0: plain
     int32_t hub_threshold = 1024;   // degree above which a vertex is aggregated in chunks; 0 = never
     int32_t profile = 0;            // time every fused launch with CUDA events
+    int32_t autotune = 1;           // time the tile-shape candidates of new stage shapes once per graph
+    int32_t exact = 0;              // reference operation order everywhere: no hub chunks, no fused products
 };
 
 struct CountStats {

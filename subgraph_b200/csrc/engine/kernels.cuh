@@ -8,6 +8,9 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <utility>
+#include <vector>
+
 #include "stage.cuh"
 
 namespace sg {
@@ -32,36 +35,26 @@ void launch_remap(int32_t V, const int32_t *old_off, const int32_t *old_adj, con
                   const int32_t *iperm, const int32_t *perm, int32_t *new_adj, cudaStream_t st);
 
 struct FusedConfig {
-    int tile_v;      // 32, 16 or 8
-    int q;           // register chunks per lane in the gather: 1, 2, 4 or 8
+    int tile_v;      // vertices per tile
+    int q;           // 16-byte chunks per gather thread
     size_t smem;     // dynamic shared memory bytes
-    int grid;        // CTAs
+    int grid;        // CTAs per SM unit (scaled by the occupancy at launch)
 };
 
-// Chooses tile size, gather grouping and shared memory for a stage (fills the
-// stage's tile_v, gather_group, ntiles and out_chunk).  Returns false when no
-// tiling fits in shared memory.
+// Chooses the tile size, CTA size, gather grouping and shared memory of a
+// stage (fills tile_v, nthreads, gather_group, gather_q, ntiles, out_chunk,
+// smem).  Returns false when no tiling fits in shared memory.
 bool plan_fused(StageDesc &d, bool fp64, int sm_count, FusedConfig &cfg);
-void launch_fused(const StageDesc &d, bool fp64, const FusedConfig &cfg, cudaStream_t st);
-
-// Aggregation of the vertices [0, hub_count) split into neighbour chunks of
-// `chunk` entries: every chunk sums sequentially into partial rows, then the
-// partial rows of a vertex are added in chunk order into hub_agg.
-struct HubArgs {
-    int32_t hub_count;
-    int32_t chunk;
-    int32_t L_a, aux_pitch;      // aux row width / pitch (elements)
-    int32_t row_pitch;           // pitch of partial and hub_agg rows
-    int32_t k_leaf;              // > 0: the aux child is one-hot, count colors (k)
-    const uint8_t *color;        // [V] internal order (k_leaf only)
-    int32_t total_chunks;
-    const int32_t *chunk_start;  // [hub_count+1] first chunk index of each hub
-    const int32_t *off;
-    const int32_t *adj;
-    const void *aux;
-    void *partial;               // [total_chunks][aux_pitch]
-    void *hub_agg;               // [hub_count][aux_pitch]
+struct TileShape {
+    int tile_v;      // vertices per tile
+    int threads;     // CTA size
+    int packed;      // packed FP32x2 eMA (32-vertex tiles)
 };
+// Sets an explicit shape (the autotuner's candidates); false when it does not fit.
+bool set_shape(StageDesc &d, bool fp64, const TileShape &shape);
+// The shapes the autotuner times for a stage.
+std::vector<TileShape> candidate_shapes(const StageDesc &d, bool fp64);
+void launch_fused(const StageDesc &d, bool fp64, const FusedConfig &cfg, cudaStream_t st);
 void launch_hub(const HubArgs &h, bool fp64, int sm_count, cudaStream_t st);
 
 void launch_root_reduce(const double *partial, int32_t n, double scale, double *out, cudaStream_t st);

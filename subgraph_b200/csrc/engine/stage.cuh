@@ -22,23 +22,53 @@ struct StageDesc {
     int32_t is_root;                   // sub 0: per-vertex root values, no table
     int32_t scaled;                    // first non-bottom sub: x 1e-12 through FP64
     int32_t root_float;                // isPruned=0: root accumulated in FP32
-    int32_t gather_group;              // lanes per vertex in the gather (power of 2)
+    // launch shape (filled by plan_fused / the autotuner)
     int32_t tile_v;                    // vertices per tile
+    int32_t nthreads;                  // CTA size (256 or 512)
+    int32_t gather_group;              // threads per vertex in the aggregation
+    int32_t gather_q;                  // 16-byte column chunks per thread (1, 2 or 4)
     int32_t ntiles;
     int32_t out_chunk;                 // outputs staged in shared memory per pass
-    int32_t hub_count;                 // vertices [0, hub_count) read hub_agg
-    int32_t hub_pitch;                 // row pitch of hub_agg
+    size_t smem;                       // dynamic shared memory bytes
+    // vertices [0, hub_count) are aggregated by the hub kernel in neighbour
+    // chunks; their partial rows are added here in chunk order
+    int32_t hub_count;
+    int32_t hub_pitch;                 // row pitch of hub_partial
+    const int32_t *hub_chunk_start;    // [hub_count+1]
+    const void *hub_partial;           // [chunks][hub_pitch]
     const void *main;
     const void *aux;
     void *out;
-    const uint32_t *split;             // [L_s][S] (main col | aux col << 16), by output column
+    const uint32_t *split;             // [S][split_stride] (main col | aux col << 16) per (split, output column)
+    int32_t split_stride;              // L_s rounded up to a multiple of 4
+    // packed eMA (FP32, 32-vertex tiles, two vertices per lane): shared rows of
+    // kPackedRow floats and the split table as byte offsets into shared memory
+    int32_t packed;
+    const uint32_t *aoff;              // [S][split_stride] aggregate row byte offset
+    const uint32_t *moff;              // [S][split_stride] main row byte offset
     const int16_t *rem;                // [L_s][k] main-leaf: aux column of set\{c}, or -1
     const uint8_t *color;              // [V] internal order
     const int32_t *off;                // [V+1]
     const int32_t *adj;                // [nnz]
-    const void *hub_agg;               // [hub_count][aux_pitch] precomputed aggregation
     double *root_partial;              // [ntiles]
     double *root_vertex;               // [V] optional (internal order)
+};
+
+// Aggregation of the vertices [0, hub_count) in neighbour chunks of `chunk`
+// entries; one item per (vertex, chunk) writes a partial row.
+struct HubArgs {
+    int32_t hub_count;
+    int32_t chunk;
+    int32_t L_a, aux_pitch;      // aux row width / pitch (elements)
+    int32_t row_pitch;           // pitch of the partial rows
+    int32_t k_leaf;              // > 0: the aux child is one-hot, count colors (k)
+    int32_t total_chunks;
+    const uint8_t *color;        // [V] internal order (k_leaf only)
+    const int32_t *chunk_start;  // [hub_count+1] first chunk index of each hub
+    const int32_t *off;
+    const int32_t *adj;
+    const void *aux;
+    void *partial;               // [total_chunks][row_pitch]
 };
 
 }  // namespace sg

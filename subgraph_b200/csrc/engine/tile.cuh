@@ -1,0 +1,494 @@
+// Device bodies of the counting step, shared by the per-stage kernels and the
+// persistent batched kernel.
+//
+// Arithmetic follows the reference's CPU code operation by operation (one
+// lane sums one aggregated column over a vertex's neighbours in list order;
+// every eMA product is accumulated in split order with separately rounded
+// multiply and add), so vertices aggregated in one piece give the reference's
+// FP32 values bit for bit (CSCGraph.hpp:242-307, DataTableColMajor.cpp:346-400).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "stage.cuh"
+
+namespace sg {
+
+__device__ __forceinline__ float ema_step(float acc, float agg, float mainv, bool scaled)
+{
+    if (scaled) {  // dst + (a * (double)b) * scale, rounded to float (DataTableColMajor.cpp:369)
+        const double p = __dmul_rn(__dmul_rn((double)agg, (double)mainv), (double)1.0e-12f);
+        return __double2float_rn(__dadd_rn((double)acc, p));
+    }
+    return __fadd_rn(acc, __fmul_rn(agg, mainv));   // dst + a*b without contraction (:492-493)
+}
+__device__ __forceinline__ double ema_step(double acc, double agg, double mainv, bool)
+{
+    return __dadd_rn(acc, __dmul_rn(agg, mainv));
+}
+// main is one-hot: the single non-zero split product is agg * 1
+__device__ __forceinline__ float leaf_value(float agg, bool scaled)
+{
+    return scaled ? __double2float_rn(__dmul_rn((double)agg, (double)1.0e-12f)) : agg;
+}
+__device__ __forceinline__ double leaf_value(double agg, bool) { return agg; }
+
+template <typename T> struct Chunk;
+template <> struct Chunk<float> {
+    using type = float4;
+    static constexpr int n = 4;
+    __device__ static float get(const float4 &v, int i) { return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w; }
+    __device__ static void add(float4 &a, const float4 &b)
+    {
+        a.x = __fadd_rn(a.x, b.x); a.y = __fadd_rn(a.y, b.y); a.z = __fadd_rn(a.z, b.z); a.w = __fadd_rn(a.w, b.w);
+    }
+    __device__ static float4 zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+};
+template <> struct Chunk<double> {
+    using type = double2;
+    static constexpr int n = 2;
+    __device__ static double get(const double2 &v, int i) { return i == 0 ? v.x : v.y; }
+    __device__ static void add(double2 &a, const double2 &b) { a.x = __dadd_rn(a.x, b.x); a.y = __dadd_rn(a.y, b.y); }
+    __device__ static double2 zero() { return make_double2(0.0, 0.0); }
+};
+
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+
+// Row stride (floats) of the aggregate and main rows in the packed layout: 32
+// vertices plus 2 so that the 16 float2 of a half-warp cover all 32 banks.
+constexpr int kPackedRow = 34;
+
+// Shared-memory layout of a tile: [La_rows][RS] aggregate, [Lm_rows][RS] main
+// rows (RS = TV+1, or kPackedRow for the packed eMA), [out_chunk][TV+1]
+// output staging, then TV doubles (root values) on a 16-byte boundary.
+template <typename T>
+__host__ __device__ inline size_t tile_smem_bytes(int La_rows, int Lm_rows, int out_chunk, int tv, bool packed)
+{
+    const size_t rs = packed ? (size_t)kPackedRow : (size_t)(tv + 1);
+    size_t b = (((size_t)(La_rows + Lm_rows) * rs + (size_t)out_chunk * (size_t)(tv + 1)) * sizeof(T) + 15) & ~(size_t)15;
+    return b + (size_t)tv * sizeof(double);
+}
+
+// packed FP32x2 arithmetic (sm_100a): two independent lanes, each rounded
+// like __fmul_rn / __fadd_rn
+__device__ __forceinline__ unsigned long long mul2_rn(unsigned long long a, unsigned long long b)
+{
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ unsigned long long add2_rn(unsigned long long a, unsigned long long b)
+{
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// ---------------------------------------------------------------------------
+// One tile of one stage: TV consecutive (degree-ordered) vertices.
+//   A. aggregation of the aux child's rows over each vertex's neighbours into
+//      shared memory, transposed [column][vertex]: `gather_group` threads per
+//      vertex, each owning gather_q 16-byte column chunks, neighbour ids and
+//      rows fetched in batches of U before they are added (memory-level
+//      parallelism without reordering the sums).  A one-hot aux child becomes
+//      a per-color neighbour count.  Hub vertices add their partial rows.
+//   B. the main child's rows of the tile, transposed the same way.
+//   C. eMA.  Non-one-hot main: lanes = vertices, one output column per lane
+//      group, split pairs as warp-uniform words, results staged and written
+//      as contiguous rows.  One-hot main: each output is one aggregated
+//      column (or zero), written directly as contiguous rows.  Root: a value
+//      per vertex, reduced over the tile in a fixed order.
+// The aggregate never leaves the chip.
+// ---------------------------------------------------------------------------
+template <typename T, int NT, int Q, bool PK = false>
+__device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigned char *smem_raw)
+{
+    using CT = Chunk<T>;
+    using C = typename CT::type;
+    constexpr int CH = CT::n;
+    constexpr int NW = NT / 32;
+    constexpr int U = Q == 1 ? 8 : (Q == 2 ? 4 : 2);
+    const int TV = d.tile_v;
+    const int TVP = TV + 1;
+    const int RS = PK ? kPackedRow : TVP;          // row stride of the aggregate and main rows
+    const int La_rows = d.aux_leaf ? d.k : d.L_a;
+    const int Lm_rows = d.main_leaf ? 0 : d.L_m;
+    T *agg_s = reinterpret_cast<T *>(smem_raw);
+    T *main_s = agg_s + (size_t)La_rows * RS;
+    T *out_s = main_s + (size_t)Lm_rows * RS;
+    const size_t root_off = (((size_t)(La_rows + Lm_rows) * RS + (size_t)d.out_chunk * TVP) * sizeof(T) + 15) & ~(size_t)15;
+    double *root_s = reinterpret_cast<double *>(smem_raw + root_off);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int v0 = tile * TV;
+    const int tv = min(TV, d.V - v0);
+    const bool scaled = d.scaled != 0;
+
+    // ---- A: aggregation ------------------------------------------------------
+    if (d.aux_leaf) {
+        // per-color neighbour counts, one thread per vertex (exact integers)
+        for (int vi = tid; vi < tv; vi += NT) {
+            for (int c = 0; c < d.k; ++c) agg_s[c * RS + vi] = T(0);
+            const int v = v0 + vi;
+            if (v < d.hub_count) {
+                const T *p = reinterpret_cast<const T *>(d.hub_partial);
+                const int c0 = __ldg(d.hub_chunk_start + v), c1 = __ldg(d.hub_chunk_start + v + 1);
+                for (int ch = c0; ch < c1; ++ch)
+                    for (int c = 0; c < d.k; ++c)
+                        agg_s[c * RS + vi] = add_rn(agg_s[c * RS + vi], p[(size_t)ch * d.hub_pitch + c]);
+                continue;
+            }
+            const int beg = __ldg(d.off + v), end = __ldg(d.off + v + 1);
+            int e = beg;
+            for (; e + 8 <= end; e += 8) {
+                int nb[8], cl[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) nb[u] = __ldg(d.adj + e + u);
+#pragma unroll
+                for (int u = 0; u < 8; ++u) cl[u] = __ldg(d.color + nb[u]);
+#pragma unroll
+                for (int u = 0; u < 8; ++u) agg_s[cl[u] * RS + vi] += T(1);
+            }
+            for (; e < end; ++e) agg_s[__ldg(d.color + __ldg(d.adj + e)) * RS + vi] += T(1);
+        }
+    } else {
+        const int G = d.gather_group;
+        const int grp = tid / G, lane_g = tid - grp * G;
+        const int ngrp = NT / G;
+        const int nchunk = (d.L_a + CH - 1) / CH;
+        const int rowc = d.aux_pitch / CH;
+        const C *auxc = reinterpret_cast<const C *>(d.aux);
+        if (grp < ngrp) {
+            for (int vi = grp; vi < tv; vi += ngrp) {
+                const int v = v0 + vi;
+                C acc[Q];
+                if (v < d.hub_count) {
+                    const C *p = reinterpret_cast<const C *>(d.hub_partial);
+                    const int prc = d.hub_pitch / CH;
+                    const int c0 = __ldg(d.hub_chunk_start + v), c1 = __ldg(d.hub_chunk_start + v + 1);
+#pragma unroll
+                    for (int r = 0; r < Q; ++r) {
+                        const int q = lane_g + G * r;
+                        acc[r] = CT::zero();
+                        if (q < nchunk)
+                            for (int ch = c0; ch < c1; ++ch) CT::add(acc[r], p[(size_t)ch * prc + q]);
+                    }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < Q; ++r) acc[r] = CT::zero();
+                    const int beg = __ldg(d.off + v), end = __ldg(d.off + v + 1);
+                    int e = beg;
+                    for (; e + U <= end; e += U) {
+                        int nb[U];
+#pragma unroll
+                        for (int u = 0; u < U; ++u) nb[u] = __ldg(d.adj + e + u);
+                        C x[U][Q];
+#pragma unroll
+                        for (int u = 0; u < U; ++u)
+#pragma unroll
+                            for (int r = 0; r < Q; ++r) {
+                                const int q = lane_g + G * r;
+                                x[u][r] = q < nchunk ? __ldg(auxc + (size_t)nb[u] * rowc + q) : CT::zero();
+                            }
+#pragma unroll
+                        for (int u = 0; u < U; ++u)
+#pragma unroll
+                            for (int r = 0; r < Q; ++r) CT::add(acc[r], x[u][r]);
+                    }
+                    for (; e < end; ++e) {
+                        const C *row = auxc + (size_t)__ldg(d.adj + e) * rowc;
+#pragma unroll
+                        for (int r = 0; r < Q; ++r) {
+                            const int q = lane_g + G * r;
+                            if (q < nchunk) CT::add(acc[r], __ldg(row + q));
+                        }
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < Q; ++r) {
+                    const int q = lane_g + G * r;
+                    if (q < nchunk) {
+#pragma unroll
+                        for (int i = 0; i < CH; ++i) {
+                            const int c = q * CH + i;
+                            if (c < d.L_a) agg_s[c * RS + vi] = CT::get(acc[r], i);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    // ---- B: main rows --------------------------------------------------------------
+    if (!d.main_leaf) {
+        const T *mainp = reinterpret_cast<const T *>(d.main);
+        for (int vi = warp; vi < tv; vi += NW) {
+            const T *row = mainp + (size_t)(v0 + vi) * d.main_pitch;
+            for (int c = lane; c < d.L_m; c += 32) main_s[c * RS + vi] = __ldg(row + c);
+        }
+    }
+    __syncthreads();
+
+    // ---- C: eMA ------------------------------------------------------------------------
+    const int VPW = TV < 32 ? TV : 32;       // vertices per warp instruction
+    const int OPI = 32 / VPW;                // outputs per warp instruction
+    const int VB = TV / VPW;                 // vertex blocks of the tile
+    const int lv = lane % VPW, osub = lane / VPW;
+    if (d.is_root) {
+        if (d.main_leaf) {
+            for (int vi = tid; vi < tv; vi += NT) {
+                const int cv = __ldg(d.color + v0 + vi);
+                const int r = __ldg(d.rem + cv);
+                root_s[vi] = r >= 0 ? (double)agg_s[r * RS + vi] : 0.0;
+            }
+        } else {
+            for (int b = warp; b < VB; b += NW) {
+                if (osub != 0) continue;
+                const int vi = b * VPW + lv;
+                double racc = 0.0;
+                float facc = 0.f;
+                for (int j = 0; j < d.S; ++j) {
+                    const uint32_t pk = __ldg(d.split + (size_t)j * d.split_stride);
+                    const T x = main_s[(pk & 0xffffu) * RS + vi];
+                    const T y = agg_s[(pk >> 16) * RS + vi];
+                    if (sizeof(T) == 8) racc = __dadd_rn(racc, __dmul_rn((double)y, (double)x));
+                    else if (d.root_float) facc = __fadd_rn(facc, __fmul_rn((float)y, (float)x));
+                    else racc = __dadd_rn(racc, (double)__fmul_rn((float)y, (float)x));
+                }
+                if (vi < tv) root_s[vi] = (sizeof(T) == 4 && d.root_float) ? (double)facc : racc;
+            }
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double s = 0.0;
+            for (int vi = lane; vi < tv; vi += 32) {
+                s = __dadd_rn(s, root_s[vi]);
+                if (d.root_vertex) d.root_vertex[v0 + vi] = root_s[vi];
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s = __dadd_rn(s, __shfl_down_sync(0xffffffffu, s, o));
+            if (lane == 0) d.root_partial[tile] = s;
+        }
+    } else if (d.main_leaf) {
+        // one-hot main: out[o] = agg[set(o) \ {color}] when color is in set(o)
+        T *outp = reinterpret_cast<T *>(d.out);
+        const int P = d.out_pitch;
+        for (int idx = tid; idx < tv * P; idx += NT) {
+            const int vi = idx / P, o = idx - vi * P;
+            T val = T(0);
+            if (o < d.L_s) {
+                const int cv = __ldg(d.color + v0 + vi);
+                const int r = __ldg(d.rem + o * d.k + cv);
+                if (r >= 0) val = leaf_value(agg_s[r * RS + vi], scaled);
+            }
+            outp[(size_t)(v0 + vi) * P + o] = val;
+        }
+    } else if (PK) {
+        // packed eMA: lane = pair of vertices (2p, 2p+1) x a group of 4 output
+        // columns; each operand is one 64-bit shared load at a byte offset taken
+        // from the split tables, and the products / sums are FP32x2 operations
+        // rounded like the scalar path.  A half-warp reads 16 consecutive
+        // float2 of one row: all 32 banks once.
+        T *outp = reinterpret_cast<T *>(d.out);
+        const int P = d.out_pitch;
+        const int SP4 = d.split_stride / 4;
+        const int pr = lane & 15, osub = lane >> 4;
+        const char *sb = reinterpret_cast<const char *>(smem_raw) + pr * 8;
+        for (int o0 = 0; o0 < d.L_s; o0 += d.out_chunk) {
+            const int oc = min(d.out_chunk, d.L_s - o0);
+            const int ngroups = (oc + 7) / 8;
+            for (int unit = warp; unit < ngroups; unit += NW) {
+                const int ol = (unit * 2 + osub) * 4;
+                if (ol >= oc) continue;
+                const uint4 *ap = reinterpret_cast<const uint4 *>(d.aoff + o0 + ol);
+                const uint4 *mp = reinterpret_cast<const uint4 *>(d.moff + o0 + ol);
+                unsigned long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+                int j = 0;
+                for (; j + 4 <= d.S; j += 4) {
+                    uint4 A[4], M[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        A[u] = __ldg(ap + (size_t)(j + u) * SP4);
+                        M[u] = __ldg(mp + (size_t)(j + u) * SP4);
+                    }
+                    unsigned long long pv[4][4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        pv[u][0] = mul2_rn(*reinterpret_cast<const unsigned long long *>(sb + A[u].x),
+                                           *reinterpret_cast<const unsigned long long *>(sb + M[u].x));
+                        pv[u][1] = mul2_rn(*reinterpret_cast<const unsigned long long *>(sb + A[u].y),
+                                           *reinterpret_cast<const unsigned long long *>(sb + M[u].y));
+                        pv[u][2] = mul2_rn(*reinterpret_cast<const unsigned long long *>(sb + A[u].z),
+                                           *reinterpret_cast<const unsigned long long *>(sb + M[u].z));
+                        pv[u][3] = mul2_rn(*reinterpret_cast<const unsigned long long *>(sb + A[u].w),
+                                           *reinterpret_cast<const unsigned long long *>(sb + M[u].w));
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        a0 = add2_rn(a0, pv[u][0]);
+                        a1 = add2_rn(a1, pv[u][1]);
+                        a2 = add2_rn(a2, pv[u][2]);
+                        a3 = add2_rn(a3, pv[u][3]);
+                    }
+                }
+                for (; j < d.S; ++j) {
+                    const uint4 A = __ldg(ap + (size_t)j * SP4), M = __ldg(mp + (size_t)j * SP4);
+                    a0 = add2_rn(a0, mul2_rn(*reinterpret_cast<const unsigned long long *>(sb + A.x),
+                                             *reinterpret_cast<const unsigned long long *>(sb + M.x)));
+                    a1 = add2_rn(a1, mul2_rn(*reinterpret_cast<const unsigned long long *>(sb + A.y),
+                                             *reinterpret_cast<const unsigned long long *>(sb + M.y)));
+                    a2 = add2_rn(a2, mul2_rn(*reinterpret_cast<const unsigned long long *>(sb + A.z),
+                                             *reinterpret_cast<const unsigned long long *>(sb + M.z)));
+                    a3 = add2_rn(a3, mul2_rn(*reinterpret_cast<const unsigned long long *>(sb + A.w),
+                                             *reinterpret_cast<const unsigned long long *>(sb + M.w)));
+                }
+                const unsigned long long av[4] = {a0, a1, a2, a3};
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (ol + u < oc) {
+                        out_s[(ol + u) * TVP + 2 * pr] = __uint_as_float((unsigned)(av[u] & 0xffffffffull));
+                        out_s[(ol + u) * TVP + 2 * pr + 1] = __uint_as_float((unsigned)(av[u] >> 32));
+                    }
+                }
+            }
+            __syncthreads();
+            const int ow = (o0 + oc == d.L_s) ? P - o0 : oc;
+            for (int idx = tid; idx < tv * ow; idx += NT) {
+                const int vj = idx / ow, t = idx - vj * ow;
+                outp[(size_t)(v0 + vj) * P + o0 + t] = t < oc ? out_s[t * TVP + vj] : T(0);
+            }
+            __syncthreads();
+        }
+    } else {
+        // each lane accumulates 4 consecutive output columns of its vertex at once
+        // (4 independent chains); the split table is stored [j][column] so one
+        // 16-byte warp-uniform load gives the 4 (main, aux) pairs of split j
+        T *outp = reinterpret_cast<T *>(d.out);
+        const int P = d.out_pitch;
+        const int SP = d.split_stride;
+        for (int o0 = 0; o0 < d.L_s; o0 += d.out_chunk) {
+            const int oc = min(d.out_chunk, d.L_s - o0);
+            const int ngroups = (oc + 4 * OPI - 1) / (4 * OPI);
+            for (int unit = warp; unit < VB * ngroups; unit += NW) {
+                const int b = unit % VB, og = unit / VB;
+                const int ol = (og * OPI + osub) * 4;
+                if (ol >= oc) continue;
+                const int vi = b * VPW + lv;
+                const uint4 *sp = reinterpret_cast<const uint4 *>(d.split + o0 + ol);
+                const size_t sstep = (size_t)(SP / 4);
+                T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+                int j = 0;
+                // blocks of 4 splits: the 4 split words, then the 32 operands,
+                // then the 16 multiply-adds (4 chains, each in split order)
+                for (; j + 4 <= d.S; j += 4) {
+                    uint4 pk[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) pk[u] = __ldg(sp + (size_t)(j + u) * sstep);
+                    T ag[4][4], mn[4][4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        ag[u][0] = agg_s[(pk[u].x >> 16) * RS + vi]; mn[u][0] = main_s[(pk[u].x & 0xffffu) * RS + vi];
+                        ag[u][1] = agg_s[(pk[u].y >> 16) * RS + vi]; mn[u][1] = main_s[(pk[u].y & 0xffffu) * RS + vi];
+                        ag[u][2] = agg_s[(pk[u].z >> 16) * RS + vi]; mn[u][2] = main_s[(pk[u].z & 0xffffu) * RS + vi];
+                        ag[u][3] = agg_s[(pk[u].w >> 16) * RS + vi]; mn[u][3] = main_s[(pk[u].w & 0xffffu) * RS + vi];
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        a0 = ema_step(a0, ag[u][0], mn[u][0], scaled);
+                        a1 = ema_step(a1, ag[u][1], mn[u][1], scaled);
+                        a2 = ema_step(a2, ag[u][2], mn[u][2], scaled);
+                        a3 = ema_step(a3, ag[u][3], mn[u][3], scaled);
+                    }
+                }
+                for (; j < d.S; ++j) {
+                    const uint4 pk = __ldg(sp + (size_t)j * sstep);
+                    a0 = ema_step(a0, agg_s[(pk.x >> 16) * RS + vi], main_s[(pk.x & 0xffffu) * RS + vi], scaled);
+                    a1 = ema_step(a1, agg_s[(pk.y >> 16) * RS + vi], main_s[(pk.y & 0xffffu) * RS + vi], scaled);
+                    a2 = ema_step(a2, agg_s[(pk.z >> 16) * RS + vi], main_s[(pk.z & 0xffffu) * RS + vi], scaled);
+                    a3 = ema_step(a3, agg_s[(pk.w >> 16) * RS + vi], main_s[(pk.w & 0xffffu) * RS + vi], scaled);
+                }
+                out_s[ol * TVP + vi] = a0;
+                if (ol + 1 < oc) out_s[(ol + 1) * TVP + vi] = a1;
+                if (ol + 2 < oc) out_s[(ol + 2) * TVP + vi] = a2;
+                if (ol + 3 < oc) out_s[(ol + 3) * TVP + vi] = a3;
+            }
+            __syncthreads();
+            const int ow = (o0 + oc == d.L_s) ? P - o0 : oc;   // the last chunk zero-fills the row padding
+            for (int idx = tid; idx < tv * ow; idx += NT) {
+                const int vj = idx / ow, t = idx - vj * ow;
+                outp[(size_t)(v0 + vj) * P + o0 + t] = t < oc ? out_s[t * TVP + vj] : T(0);
+            }
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// One hub item: the neighbour chunk `item` of a hub vertex, summed into a
+// partial row.  Threads are (neighbour lane r, column chunk q); lane r sums
+// the chunk's neighbours r, r+R, ... in order, and the R lane sums are added
+// in lane order: a fixed summation order.  A one-hot aux child counts colors.
+// Needs NT * 16 bytes of shared memory (the lane partials).
+// ---------------------------------------------------------------------------
+template <typename T, int NT>
+__device__ __forceinline__ void hub_item(const HubArgs &h, int item, unsigned char *smem_raw)
+{
+    using CT = Chunk<T>;
+    using C = typename CT::type;
+    constexpr int CH = CT::n;
+    int lo = 0, hi = h.hub_count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(h.chunk_start + mid) <= item) lo = mid; else hi = mid - 1;
+    }
+    const int v = lo;
+    const int c = item - __ldg(h.chunk_start + v);
+    const int beg = __ldg(h.off + v) + c * h.chunk;
+    const int end = min(__ldg(h.off + v + 1), beg + h.chunk);
+    T *prow = reinterpret_cast<T *>(h.partial) + (size_t)item * h.row_pitch;
+    if (h.k_leaf) {
+        uint32_t *cnt = reinterpret_cast<uint32_t *>(smem_raw);
+        if (threadIdx.x < 32) cnt[threadIdx.x] = 0;
+        __syncthreads();
+        for (int e = beg + (int)threadIdx.x; e < end; e += NT) atomicAdd(&cnt[__ldg(h.color + __ldg(h.adj + e))], 1u);
+        __syncthreads();
+        if ((int)threadIdx.x < h.k_leaf) prow[threadIdx.x] = (T)cnt[threadIdx.x];
+        __syncthreads();
+        return;
+    }
+    C *lanes = reinterpret_cast<C *>(smem_raw);
+    const int nchunk = (h.L_a + CH - 1) / CH;
+    const int rowc = h.aux_pitch / CH;
+    const C *auxc = reinterpret_cast<const C *>(h.aux);
+    for (int base = 0; base < nchunk; base += NT) {
+        const int cols = min(NT, nchunk - base);
+        const int R = NT / cols;
+        const int r = threadIdx.x / cols, q = base + (int)threadIdx.x - r * cols;
+        C acc = CT::zero();
+        if (r < R) {
+            int e = beg + r;
+            for (; e + 3 * R < end; e += 4 * R) {
+                const C x0 = __ldg(auxc + (size_t)__ldg(h.adj + e) * rowc + q);
+                const C x1 = __ldg(auxc + (size_t)__ldg(h.adj + e + R) * rowc + q);
+                const C x2 = __ldg(auxc + (size_t)__ldg(h.adj + e + 2 * R) * rowc + q);
+                const C x3 = __ldg(auxc + (size_t)__ldg(h.adj + e + 3 * R) * rowc + q);
+                CT::add(acc, x0);
+                CT::add(acc, x1);
+                CT::add(acc, x2);
+                CT::add(acc, x3);
+            }
+            for (; e < end; e += R) CT::add(acc, __ldg(auxc + (size_t)__ldg(h.adj + e) * rowc + q));
+            lanes[threadIdx.x] = acc;
+        }
+        __syncthreads();
+        if ((int)threadIdx.x < cols) {
+            C s = lanes[threadIdx.x];
+            for (int rr = 1; rr < R; ++rr) CT::add(s, lanes[rr * cols + threadIdx.x]);
+            reinterpret_cast<C *>(prow)[base + threadIdx.x] = s;
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace sg
