@@ -159,6 +159,22 @@ sg_status sg_debug_sub_table(sg_graph g, sg_plan p, uint32_t seed, int32_t mode,
 sg_status sg_debug_root(sg_graph g, sg_plan p, uint32_t seed, int32_t mode, int32_t hub_threshold,
                         double *root, double *raw);
 
+/* The coloring of sg_colors for callers that cannot allocate device memory
+ * (no counterpart in the reference).  Frameworks that reserve all GPU memory
+ * in their own pool, and pipelines that cannot afford the device
+ * synchronisation an allocation implies, pass the output buffer themselves:
+ * d_colors is a DEVICE array of V int32 written with rand() % k after
+ * srand(seed), in vertex order, on `stream` (a cudaStream_t; NULL = legacy
+ * stream).  The call allocates nothing: its scratch (the glibc stream's
+ * jump-ahead tables, 8.3 MB) is a fixed array in the library that every GPU
+ * that loads the library keeps until the process exits; V is limited to 2^26
+ * and larger V is rejected with SG_ERR_INVALID.  The first call on a device
+ * looks up that array's address on the device and should come before any
+ * stream capture.  Every call rewrites the tables it reads and waits for
+ * that upload; calls that overlap on the GPU (other threads, other streams)
+ * share the array and race. */
+sg_status sg_colors_noalloc(int32_t V, int32_t k, uint32_t seed, int32_t *d_colors, void *stream);
+
 /* ---- CountMat mirror ---------------------------------------------------- */
 
 /* CountMat::initialization (CountMat.hpp:32-33).  Exactly one of the graphs is

@@ -32,7 +32,7 @@ EXPORTS = [
     "sg_plan_tables", "sg_plan_automorphisms", "sg_plan_sub_edges",
     "sg_graph_create", "sg_graph_destroy", "sg_graph_info",
     "sg_count_opts_default", "sg_count", "sg_estimate",
-    "sg_colors", "sg_debug_sub_table", "sg_debug_root",
+    "sg_colors", "sg_debug_sub_table", "sg_debug_root", "sg_colors_noalloc",
     "sg_countmat_create", "sg_countmat_destroy", "sg_countmat_initialization",
     "sg_countmat_set_seed", "sg_countmat_compute", "sg_countmat_raw",
 ]
@@ -99,6 +99,7 @@ def lib() -> ctypes.CDLL:
         "sg_colors": ([vp, i32, u32, vp], i32),
         "sg_debug_sub_table": ([vp, vp, u32, i32, i32, i32, vp], i32),
         "sg_debug_root": ([vp, vp, u32, i32, i32, vp, P(d)], i32),
+        "sg_colors_noalloc": ([i32, i32, u32, vp, vp], i32),
         "sg_countmat_create": ([pp], i32),
         "sg_countmat_destroy": ([vp], None),
         "sg_countmat_initialization": ([vp, vp, vp, i32, i32, i32, i32, i32, i32], i32),

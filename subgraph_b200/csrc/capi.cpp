@@ -56,6 +56,10 @@ template <typename T> T *dup_array(const std::vector<T> &v)
 
 }  // namespace
 
+namespace sg {
+void set_last_error(const std::string &msg) { t_err = msg; }
+}
+
 extern "C" {
 
 const char *sg_last_error(void) { return t_err.c_str(); }
