@@ -121,6 +121,11 @@ typedef struct {
                                fused multiply-add): per-vertex values bit-identical to
                                the reference; otherwise products may be fused (one
                                rounding) and hub neighbour lists summed in chunks */
+    int32_t wait_limit_ms;  /* batched form: how long a work item may wait for its inputs
+                               before the call fails with SG_ERR_TIMEOUT (0 = 2000 ms) */
+    int32_t test_unsatisfiable_wait; /* test hook: in the batched form the first fused stage
+                               also waits on a counter nothing increments, so the call
+                               must end with SG_ERR_TIMEOUT */
 } sg_count_opts;
 
 typedef struct {

@@ -315,6 +315,8 @@ sg_status sg_count(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw, s
     co.profile = o->profile;
     co.autotune = o->no_autotune ? 0 : 1;
     co.exact = o->exact ? 1 : 0;
+    co.wait_limit_ms = o->wait_limit_ms;
+    co.test_unsatisfiable_wait = o->test_unsatisfiable_wait;
     sg::CountStats cs;
     sg_status st = from(sg::count(*g->g, p->p, co, raw, &cs));
     if (st) return st;

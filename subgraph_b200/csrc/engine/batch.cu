@@ -1,0 +1,150 @@
+// The batched form: one persistent launch runs every (coloring, sub-template)
+// stage of a batch of colorings from a work queue.
+//
+// Items are numbered stage by stage in an order where every stage comes after
+// the stages it reads (sub-templates in processing order, colorings
+// interleaved), so a claimed item only ever waits for lower-numbered items,
+// which were claimed by CTAs that are already running: the queue cannot
+// deadlock.  A stage's completion is an item counter; a CTA's thread 0 waits
+// on the counters of the stage's inputs with acquire loads, bounded by a
+// cycle budget after which it raises the batch's error flag (every later wait
+// then returns at once and the host reports SG_ERR_TIMEOUT).  Tables produced
+// inside the launch are read through L2 (fused_tile<..., COH = true>).
+#include "kernels.cuh"
+#include "tile.cuh"
+
+namespace sg {
+
+__device__ __forceinline__ int ld_acquire(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ void batch_fused(const StageDesc &d, int tile, unsigned char *smem)
+{
+    constexpr int NT = kBatchThreads;
+    if (sizeof(T) == 4 && d.packed) {
+        switch (d.gather_q) {
+        case 1: fused_tile<T, NT, 1, true, true>(d, tile, smem); break;
+        case 2: fused_tile<T, NT, 2, true, true>(d, tile, smem); break;
+        default: fused_tile<T, NT, 4, true, true>(d, tile, smem); break;
+        }
+    } else {
+        switch (d.gather_q) {
+        case 1: fused_tile<T, NT, 1, false, true>(d, tile, smem); break;
+        case 2: fused_tile<T, NT, 2, false, true>(d, tile, smem); break;
+        default: fused_tile<T, NT, 4, false, true>(d, tile, smem); break;
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBatchThreads, 1)
+    k_persistent(const BatchStage *__restrict__ stages, int nstages, int total_items, int *done, BatchCtl *ctl,
+                 long long wait_cycles)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ BatchStage st;
+    __shared__ int s_item, s_stage, s_skip;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(&ctl->next_item, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= total_items) break;
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = nstages - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (stages[mid].first_item <= item) lo = mid; else hi = mid - 1;
+            }
+            s_stage = lo;
+            const BatchStage &bs = stages[lo];
+            for (int q = 0; q < bs.ndeps; ++q) {
+                const int dep = bs.deps[q];
+                const int need = stages[dep].nitems;
+                const long long t0 = clock64();
+                while (ld_acquire(done + dep) < need) {
+                    if (ld_acquire(&ctl->error)) break;
+                    if (clock64() - t0 > wait_cycles) {
+                        if (atomicCAS(&ctl->error, 0, 1) == 0) ctl->error_stage = lo;
+                        break;
+                    }
+                    __nanosleep(256);
+                }
+            }
+            s_skip = ld_acquire(&ctl->error);
+        }
+        __syncthreads();
+        {   // the stage descriptor into shared memory
+            const int *src = reinterpret_cast<const int *>(stages + s_stage);
+            int *dst = reinterpret_cast<int *>(&st);
+            for (int i = threadIdx.x; i < (int)(sizeof(BatchStage) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+        }
+        __syncthreads();
+        if (!s_skip) {
+            const int local = item - st.first_item;
+            if (st.kind == kStageHub) {
+                hub_item<T, kBatchThreads, true>(st.h, local, smem_raw);
+            } else {
+                const int t0 = local * st.tiles_per_item;
+                const int t1 = min(t0 + st.tiles_per_item, st.d.ntiles);
+                for (int t = t0; t < t1; ++t) batch_fused<T>(st.d, t, smem_raw);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(done + s_stage, 1);
+        }
+    }
+}
+
+// per-slot root sums of a batch (one CTA per coloring slot), FP64 Kahan in a
+// fixed order like k_root_reduce
+__global__ void k_root_reduce_slots(const double *__restrict__ partial, int64_t slot_stride, int32_t n, double scale,
+                                    double *out)
+{
+    __shared__ double ss[256], cc[256];
+    const double *p = partial + (size_t)blockIdx.x * slot_stride;
+    double s = 0.0, c = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double y = __dadd_rn(p[i], -c);
+        const double t = __dadd_rn(s, y);
+        c = __dadd_rn(__dadd_rn(t, -s), -y);
+        s = t;
+    }
+    ss[threadIdx.x] = s;
+    cc[threadIdx.x] = c;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            ss[threadIdx.x] = __dadd_rn(ss[threadIdx.x], ss[threadIdx.x + w]);
+            cc[threadIdx.x] = __dadd_rn(cc[threadIdx.x], cc[threadIdx.x + w]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = __dmul_rn(__dadd_rn(ss[0], -cc[0]), scale);
+}
+
+cudaError_t launch_persistent(const BatchStage *stages, int nstages, int total_items, int *done, BatchCtl *ctl,
+                              long long wait_cycles, size_t smem, bool fp64, int sm_count, cudaStream_t st)
+{
+    auto go = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<sm_count, kBatchThreads, smem, st>>>(stages, nstages, total_items, done, ctl, wait_cycles);
+    };
+    if (fp64) go(k_persistent<double>);
+    else go(k_persistent<float>);
+    return cudaGetLastError();
+}
+
+void launch_root_reduce_slots(const double *partial, int64_t slot_stride, int32_t n, double scale, double *out,
+                              int nslots, cudaStream_t st)
+{
+    if (nslots > 0) k_root_reduce_slots<<<nslots, 256, 0, st>>>(partial, slot_stride, n, scale, out);
+}
+
+}  // namespace sg

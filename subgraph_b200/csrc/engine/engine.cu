@@ -98,6 +98,7 @@ struct Workspace {
     size_t chunk_start_bytes = 0;
     double *root_vertex = nullptr;
     size_t root_vertex_bytes = 0;
+    uint64_t generation = 0;   // bumped whenever a buffer above is re-allocated
 };
 
 struct DevicePlanTables {
@@ -106,10 +107,36 @@ struct DevicePlanTables {
     std::vector<uint32_t *> aoff, moff;  // per sub: packed-layout byte offsets (FP32)
 };
 
+// The work queue of one batch shape (plan, slots, mode, hubs), built once per
+// graph and replayed as a CUDA graph.
+struct BatchPlan {
+    int slots = 0;
+    int nstages = 0, total_items = 0;
+    int root_tiles = 0;
+    size_t smem = 0;
+    BatchStage *d_stages = nullptr;
+    int *d_done = nullptr;         // [nstages] completed items
+    BatchCtl *d_ctl = nullptr;
+    double *d_raw = nullptr;       // [slots] raw counts of the batch
+    void *d_hub = nullptr;         // hub partial rows, one region per (slot, sub)
+    cudaGraphExec_t exec = nullptr;
+    uint64_t generation = 0;       // workspace generation the pointers belong to
+    std::vector<BatchStage> host_stages;
+};
+
+void free_batch(BatchPlan &b, cudaStream_t stream)
+{
+    if (b.exec) cudaGraphExecDestroy(b.exec);
+    for (void *p : {(void *)b.d_stages, (void *)b.d_done, (void *)b.d_ctl, (void *)b.d_raw, b.d_hub})
+        if (p) cudaFreeAsync(p, stream);
+    b = BatchPlan();
+}
+
 struct GraphState {
     Workspace ws;
     std::map<uint64_t, DevicePlanTables> plans;
     std::map<std::string, TileShape> tuned;   // stage shape -> tile shape
+    std::map<std::string, BatchPlan> batches; // batch shape -> work queue
 };
 
 std::string shape_key(const StageDesc &d, bool fp64, int hubs)
@@ -142,9 +169,12 @@ void keep_pool_memory(int device)
     }
 }
 
+uint64_t g_grow_count = 0;   // re-allocations so far (the workspace generation)
+
 Status grow(void **p, size_t *have, size_t need, cudaStream_t st)
 {
     if (need <= *have) return Status::ok();
+    ++g_grow_count;
     if (*p) cudaFreeAsync(*p, st);
     *p = nullptr;
     *have = 0;
@@ -247,6 +277,7 @@ DeviceGraph::~DeviceGraph()
                 for (auto *p : kv.second.aoff) if (p) cudaFreeAsync(p, stream);
                 for (auto *p : kv.second.moff) if (p) cudaFreeAsync(p, stream);
             }
+            for (auto &kv : it->second.batches) free_batch(kv.second, stream);
             g_state.erase(it);
         }
     }
@@ -428,8 +459,9 @@ void *table_ptr(RunCtx &c, int slot, int sub)
     return (char *)c.gs.ws.arena + c.arena_per_coloring * slot + (size_t)c.p.table_offset[sub] * c.g.V * c.es;
 }
 
-// One sub-template step of the coloring in color slot `slot`.
-Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t st)
+// The descriptor of one sub-template step of the coloring in color slot `slot`
+// (shape fields left for plan_fused / set_shape).
+StageDesc make_stage(RunCtx &c, int slot, int s, double *root_vertex)
 {
     const Plan &p = c.p;
     const SubTemplate &sub = p.subs[s];
@@ -465,21 +497,42 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
     d.adj = g.d_adj;
     d.root_partial = w.partial + (size_t)slot * (g.V / 8 + 2);
     d.root_vertex = root_vertex;
+    return d;
+}
+
+// The hub aggregation feeding stage d, writing its partial rows to `partial`;
+// also points d at those rows.
+HubArgs make_hub(RunCtx &c, StageDesc &d, void *partial)
+{
+    DeviceGraph &g = c.g;
+    HubArgs h{};
+    h.hub_count = c.hubs.count;
+    h.chunk = c.hubs.chunk;
+    h.L_a = d.L_a;
+    h.aux_pitch = d.aux_pitch;
+    h.row_pitch = c.hub_pitch;
+    h.k_leaf = d.aux_leaf ? c.p.k : 0;
+    h.color = d.color;
+    h.total_chunks = c.hubs.total_chunks;
+    h.chunk_start = c.gs.ws.chunk_start;
+    h.off = g.d_off;
+    h.adj = g.d_adj;
+    h.aux = d.aux;
+    h.partial = partial;
+    d.hub_count = c.hubs.count;
+    d.hub_pitch = c.hub_pitch;
+    d.hub_chunk_start = c.gs.ws.chunk_start;
+    d.hub_partial = partial;
+    return h;
+}
+
+// One sub-template step of the coloring in color slot `slot`.
+Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t st)
+{
+    DeviceGraph &g = c.g;
+    StageDesc d = make_stage(c, slot, s, root_vertex);
     if (c.hubs.count > 0) {
-        HubArgs h{};
-        h.hub_count = c.hubs.count;
-        h.chunk = c.hubs.chunk;
-        h.L_a = a.L;
-        h.aux_pitch = d.aux_pitch;
-        h.row_pitch = c.hub_pitch;
-        h.k_leaf = d.aux_leaf ? p.k : 0;
-        h.color = d.color;
-        h.total_chunks = c.hubs.total_chunks;
-        h.chunk_start = w.chunk_start;
-        h.off = g.d_off;
-        h.adj = g.d_adj;
-        h.aux = d.aux;
-        h.partial = w.hub_partial;
+        HubArgs h = make_hub(c, d, c.gs.ws.hub_partial);
         if (c.profile) {
             SG_CKS(ev_pair(c.hub_ev));
             SG_CK(cudaEventRecord(c.hub_ev.back().first, st));
@@ -487,10 +540,6 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
         launch_hub(h, c.fp64, g.sm_count, st);
         if (c.profile) SG_CK(cudaEventRecord(c.hub_ev.back().second, st));
         c.launches += 1;
-        d.hub_count = c.hubs.count;
-        d.hub_pitch = c.hub_pitch;
-        d.hub_chunk_start = w.chunk_start;
-        d.hub_partial = w.hub_partial;
     }
     FusedConfig cfg;
     if (!plan_fused(d, c.fp64, g.sm_count, cfg))
@@ -591,6 +640,226 @@ Status upload_windows(RunCtx &c, uint32_t seed_base, int n)
     return Status::ok();
 }
 
+// Tile shape of a stage in the persistent kernel (1024 threads, one CTA per SM).
+bool batch_shape(StageDesc &d, bool fp64)
+{
+    const bool heavy = !d.main_leaf && !d.is_root && (int64_t)d.S * d.L_s >= 512;
+    std::vector<TileShape> cands;
+    if (d.aux_leaf) cands = {{256, kBatchThreads, 0}, {64, kBatchThreads, 0}, {32, kBatchThreads, 0}};
+    else if (heavy) cands = {{32, kBatchThreads, 1}, {32, kBatchThreads, 0}, {16, kBatchThreads, 0}, {8, kBatchThreads, 0}};
+    else cands = {{32, kBatchThreads, 0}, {16, kBatchThreads, 0}, {8, kBatchThreads, 0}};
+    for (auto &t : cands)
+        if (set_shape(d, fp64, t)) return true;
+    return false;
+}
+
+// Builds the work queue of a batch of `slots` colorings: for every sub in
+// processing order and every slot, the hub chunks (when the graph has hubs)
+// and the fused tile groups of that (slot, sub) stage.
+Status build_batch(RunCtx &c, int slots, bool poison, BatchPlan &bp)
+{
+    const Plan &p = c.p;
+    DeviceGraph &g = c.g;
+    const int nproc = (int)p.process_order.size();
+    std::vector<int> proc_index(p.nsub(), -1);
+    for (int i = 0; i < nproc; ++i) proc_index[p.process_order[i]] = i;
+    const size_t hub_region = (size_t)c.hubs.total_chunks * (size_t)std::max(c.hub_pitch, 4) * c.es;
+    if (c.hubs.count > 0) {
+        const size_t bytes = std::max<size_t>(16, hub_region * (size_t)slots * nproc);
+        SG_CK(cudaMallocAsync(&bp.d_hub, bytes, g.stream));
+    }
+    std::vector<int> fused_stage((size_t)slots * p.nsub(), -1), hub_stage((size_t)slots * p.nsub(), -1);
+    std::vector<BatchStage> &S = bp.host_stages;
+    S.clear();
+    int item = 0;
+    size_t smem = (size_t)kBatchThreads * 16;   // hub items' lane partials
+    for (int s : p.process_order) {
+        const SubTemplate &sub = p.subs[s];
+        for (int b = 0; b < slots; ++b) {
+            StageDesc d = make_stage(c, b, s, nullptr);
+            if (c.hubs.count > 0) {
+                void *region = (char *)bp.d_hub + hub_region * ((size_t)b * nproc + proc_index[s]);
+                BatchStage hs{};
+                hs.kind = kStageHub;
+                hs.h = make_hub(c, d, region);
+                hs.first_item = item;
+                hs.nitems = c.hubs.total_chunks;
+                if (p.subs[sub.aux].size > 1) hs.deps[hs.ndeps++] = fused_stage[(size_t)b * p.nsub() + sub.aux];
+                item += hs.nitems;
+                hub_stage[(size_t)b * p.nsub() + s] = (int)S.size();
+                S.push_back(hs);
+            }
+            if (!batch_shape(d, c.fp64))
+                return Status{6, "sub-template " + std::to_string(s) + " needs more shared memory than a CTA has"};
+            BatchStage fs{};
+            fs.kind = kStageFused;
+            fs.d = d;
+            fs.tiles_per_item = std::max(1, 1024 / d.tile_v);
+            fs.first_item = item;
+            fs.nitems = (d.ntiles + fs.tiles_per_item - 1) / fs.tiles_per_item;
+            std::vector<int> deps;
+            if (p.subs[sub.main].size > 1) deps.push_back(fused_stage[(size_t)b * p.nsub() + sub.main]);
+            if (p.subs[sub.aux].size > 1) deps.push_back(fused_stage[(size_t)b * p.nsub() + sub.aux]);
+            if (c.hubs.count > 0) deps.push_back(hub_stage[(size_t)b * p.nsub() + s]);
+            // write after read: the arena gives this table the range of tables
+            // already consumed; their consumers may still be reading it
+            if (s != 0) {
+                const int64_t lo = p.table_offset[s], hi = lo + p.table_pitch[s];
+                for (int x : p.process_order) {
+                    if (x == s) break;
+                    const int par = p.subs[x].parent;
+                    if (x == 0 || par < 0 || par >= p.nsub() || proc_index[par] >= proc_index[s]) continue;
+                    const int64_t xlo = p.table_offset[x], xhi = xlo + p.table_pitch[x];
+                    if (xlo < hi && lo < xhi) {
+                        const int dep = fused_stage[(size_t)b * p.nsub() + par];
+                        if (std::find(deps.begin(), deps.end(), dep) == deps.end()) deps.push_back(dep);
+                    }
+                }
+            }
+            if ((int)deps.size() > kBatchMaxDeps)
+                return Status{6, "sub-template " + std::to_string(s) + " needs more queue dependencies than a stage holds"};
+            for (int dep : deps) fs.deps[fs.ndeps++] = dep;
+            item += fs.nitems;
+            smem = std::max(smem, d.smem);
+            if (s == 0) bp.root_tiles = d.ntiles;
+            fused_stage[(size_t)b * p.nsub() + s] = (int)S.size();
+            S.push_back(fs);
+        }
+    }
+    if (poison) {
+        // test hook: a stage no item belongs to; the first fused stage waits on it
+        BatchStage ds{};
+        ds.kind = kStageFused;
+        ds.first_item = item;
+        ds.nitems = 1;
+        for (auto &st : S)
+            if (st.kind == kStageFused && st.ndeps < kBatchMaxDeps) { st.deps[st.ndeps++] = (int)S.size(); break; }
+        S.push_back(ds);
+    }
+    bp.slots = slots;
+    bp.nstages = (int)S.size();
+    bp.total_items = item;
+    bp.smem = smem;
+    SG_CK(cudaMallocAsync(&bp.d_stages, sizeof(BatchStage) * S.size(), g.stream));
+    SG_CK(cudaMemcpyAsync(bp.d_stages, S.data(), sizeof(BatchStage) * S.size(), cudaMemcpyHostToDevice, g.stream));
+    SG_CK(cudaMallocAsync(&bp.d_done, sizeof(int) * S.size(), g.stream));
+    SG_CK(cudaMallocAsync(&bp.d_ctl, sizeof(BatchCtl), g.stream));
+    SG_CK(cudaMallocAsync(&bp.d_raw, sizeof(double) * slots, g.stream));
+    SG_CK(cudaStreamSynchronize(g.stream));
+    return Status::ok();
+}
+
+// The launches of one batch: colors of every slot, the queue reset, the
+// persistent kernel and the per-slot root sums.
+Status enqueue_batch(RunCtx &c, BatchPlan &bp, long long wait_cycles, cudaStream_t st)
+{
+    SG_CKS(launch_colors(c, 0, 0, bp.slots, st));
+    SG_CK(cudaMemsetAsync(bp.d_done, 0, sizeof(int) * bp.nstages, st));
+    SG_CK(cudaMemsetAsync(bp.d_ctl, 0, sizeof(BatchCtl), st));
+    SG_CK(launch_persistent(bp.d_stages, bp.nstages, bp.total_items, bp.d_done, bp.d_ctl, wait_cycles, bp.smem,
+                            c.fp64, c.g.sm_count, st));
+    const double scale = c.mode == kModeReference ? 1.0e12 : 1.0;
+    launch_root_reduce_slots(c.gs.ws.partial, (int64_t)(c.g.V / 8 + 2), bp.root_tiles, scale, bp.d_raw, bp.slots, st);
+    SG_CK(cudaGetLastError());
+    c.launches += 3;
+    return Status::ok();
+}
+
+// Batched form: `batch` colorings per persistent launch, each batch replayed
+// from a CUDA graph.  Slots are admitted by free device memory.
+Status count_batched(RunCtx &c, const CountOptions &o, double *raw, CountStats *stats)
+{
+    DeviceGraph &g = c.g;
+    const Plan &p = c.p;
+    cudaStream_t st = g.stream;
+    const size_t V = (size_t)g.V;
+    int slots = std::min(o.batch, o.n_colorings);
+    {
+        // admission: a slot needs its table arena, colors, root partials and hub rows
+        size_t free_b = 0, total_b = 0;
+        SG_CK(cudaMemGetInfo(&free_b, &total_b));
+        const size_t held = c.gs.ws.arena_bytes;   // reused by the batch
+        const size_t per_slot = (size_t)p.arena_units * V * c.es + V + 8 * (V / 8 + 2) +
+                                (size_t)c.hubs.total_chunks * (size_t)std::max(c.hub_pitch, 4) * c.es *
+                                    p.process_order.size();
+        const size_t budget = (size_t)((double)(free_b + held) * 0.9);
+        const int fit = per_slot ? (int)std::min<size_t>(budget / per_slot, (size_t)slots) : slots;
+        if (fit < 1) return Status{2, "not enough device memory for one coloring's tables"};
+        slots = std::min(slots, fit);
+    }
+    SG_CKS(prepare(c, slots, o.n_colorings));
+    // any re-allocation since a queue was built (by any call) may have moved its buffers
+    c.gs.ws.generation = g_grow_count;
+    // queues built on buffers that have since moved are stale
+    for (auto it = c.gs.batches.begin(); it != c.gs.batches.end();) {
+        if (it->second.generation != c.gs.ws.generation) {
+            free_batch(it->second, st);
+            it = c.gs.batches.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    const long long wait_cycles = (long long)(o.wait_limit_ms > 0 ? o.wait_limit_ms : 2000) * 2000000LL;
+    cudaEvent_t e0, e1;
+    SG_CK(cudaEventCreate(&e0));
+    SG_CK(cudaEventCreate(&e1));
+    double total_ms = 0;
+    for (int c0 = 0; c0 < o.n_colorings; c0 += slots) {
+        const int nb = std::min(slots, o.n_colorings - c0);
+        char key[200];
+        std::snprintf(key, sizeof key, "%llu/%d/%d/%d/%d/%d", (unsigned long long)p.uid, nb, c.mode, c.hubs.count,
+                      (int)c.exact, o.test_unsatisfiable_wait);
+        auto it = c.gs.batches.find(key);
+        if (it == c.gs.batches.end()) {
+            BatchPlan bp;
+            bp.generation = c.gs.ws.generation;
+            SG_CKS(build_batch(c, nb, o.test_unsatisfiable_wait != 0, bp));
+            it = c.gs.batches.emplace(key, std::move(bp)).first;
+        }
+        BatchPlan &bp = it->second;
+        SG_CKS(upload_windows(c, o.seed_base + (uint32_t)c0, nb));
+        SG_CK(cudaEventRecord(e0, st));
+        if (!bp.exec) {
+            // first use: run the launches directly (sets kernel attributes), then capture them
+            SG_CKS(enqueue_batch(c, bp, wait_cycles, st));
+            SG_CK(cudaStreamSynchronize(st));
+            cudaGraph_t graph;
+            SG_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            Status cs = enqueue_batch(c, bp, wait_cycles, st);
+            cudaError_t ce = cudaStreamEndCapture(st, &graph);
+            if (cs.code) return cs;
+            SG_CK(ce);
+            SG_CK(cudaGraphInstantiate(&bp.exec, graph, 0));
+            cudaGraphDestroy(graph);
+            c.launches -= 3;   // the captured launches are counted when replayed
+        } else {
+            SG_CK(cudaGraphLaunch(bp.exec, st));
+            c.launches += 3;
+        }
+        SG_CK(cudaEventRecord(e1, st));
+        SG_CK(cudaMemcpyAsync(c.gs.ws.raw + c0, bp.d_raw, sizeof(double) * nb, cudaMemcpyDeviceToDevice, st));
+        BatchCtl ctl{};
+        SG_CK(cudaMemcpyAsync(&ctl, bp.d_ctl, sizeof ctl, cudaMemcpyDeviceToHost, st));
+        SG_CK(cudaStreamSynchronize(st));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        total_ms += ms;
+        if (ctl.error)
+            return Status{4, "batched queue: a work item waited longer than the limit for its inputs (stage " +
+                                 std::to_string(ctl.error_stage) + ")"};
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    SG_CK(cudaMemcpyAsync(raw, c.gs.ws.raw, sizeof(double) * o.n_colorings, cudaMemcpyDeviceToHost, st));
+    SG_CK(cudaStreamSynchronize(st));
+    if (stats) {
+        stats->device_ms = total_ms;
+        stats->kernel_launches = c.launches;
+        stats->table_bytes = (int64_t)(c.arena_per_coloring * slots);
+    }
+    return Status::ok();
+}
+
 }  // namespace
 
 Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, CountStats *stats)
@@ -606,6 +875,7 @@ Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, 
     c.hubs = plan_hubs(g, c.exact ? 0 : o.hub_threshold);
     c.profile = o.profile != 0;
     c.autotune = o.autotune != 0;
+    if (o.batch > 0) return count_batched(c, o, raw, stats);
     const int slots = 1;
     SG_CKS(prepare(c, slots, o.n_colorings));
     SG_CKS(upload_windows(c, o.seed_base, o.n_colorings));

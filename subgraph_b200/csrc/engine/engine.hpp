@@ -53,6 +53,8 @@ struct CountOptions {
     int32_t profile = 0;            // time every fused launch with CUDA events
     int32_t autotune = 1;           // time the tile-shape candidates of new stage shapes once per graph
     int32_t exact = 0;              // reference operation order everywhere: no hub chunks, no fused products
+    int32_t wait_limit_ms = 0;      // batched queue: time a dependency wait may take (0 = 2000 ms)
+    int32_t test_unsatisfiable_wait = 0;   // test hook: the first fused stage waits on a counter nothing sets
 };
 
 struct CountStats {

@@ -59,4 +59,10 @@ void launch_hub(const HubArgs &h, bool fp64, int sm_count, cudaStream_t st);
 
 void launch_root_reduce(const double *partial, int32_t n, double scale, double *out, cudaStream_t st);
 
+// the batched form (batch.cu)
+cudaError_t launch_persistent(const BatchStage *stages, int nstages, int total_items, int *done, BatchCtl *ctl,
+                              long long wait_cycles, size_t smem, bool fp64, int sm_count, cudaStream_t st);
+void launch_root_reduce_slots(const double *partial, int64_t slot_stride, int32_t n, double scale, double *out,
+                              int nslots, cudaStream_t st);
+
 }  // namespace sg

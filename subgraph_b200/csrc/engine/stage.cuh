@@ -71,4 +71,32 @@ struct HubArgs {
     void *partial;               // [total_chunks][row_pitch]
 };
 
+// ---------------------------------------------------------------------------
+// The batched form's work queue: one entry per (coloring slot, sub-template)
+// stage, hub chunks and fused tile groups as items.
+// ---------------------------------------------------------------------------
+constexpr int kBatchThreads = 1024;   // one persistent CTA per SM
+// producers (main, aux, hub chunks) plus the readers of earlier tables whose
+// arena range a stage overwrites; trees of up to 16 vertices need at most 9
+constexpr int kBatchMaxDeps = 12;
+constexpr int kStageHub = 0, kStageFused = 1;
+
+struct BatchStage {
+    int32_t kind;            // kStageHub or kStageFused
+    int32_t first_item;      // items [first_item, first_item + nitems)
+    int32_t nitems;
+    int32_t tiles_per_item;  // fused: consecutive tiles per item
+    int32_t ndeps;
+    int32_t deps[kBatchMaxDeps];   // stages that must be complete (all their items)
+    StageDesc d;
+    HubArgs h;
+};
+
+struct BatchCtl {
+    int32_t next_item;       // the queue head
+    int32_t error;           // set when a dependency wait ran out of time
+    int32_t error_stage;
+    int32_t pad;
+};
+
 }  // namespace sg

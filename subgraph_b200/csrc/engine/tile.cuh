@@ -52,6 +52,12 @@ template <> struct Chunk<double> {
     __device__ static double2 zero() { return make_double2(0.0, 0.0); }
 };
 
+// Loads of count tables and partial rows.  The per-stage kernels read tables
+// written by earlier launches (read-only for the launch: the non-coherent
+// path); the persistent kernel reads tables produced inside the same launch,
+// so it loads them through L2 (ld.global.cg), the point of coherence.
+template <bool COH, typename P> __device__ __forceinline__ P ld_tab(const P *p) { return COH ? __ldcg(p) : __ldg(p); }
+
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 
@@ -101,7 +107,7 @@ __device__ __forceinline__ unsigned long long add2_rn(unsigned long long a, unsi
 //      per vertex, reduced over the tile in a fixed order.
 // The aggregate never leaves the chip.
 // ---------------------------------------------------------------------------
-template <typename T, int NT, int Q, bool PK = false>
+template <typename T, int NT, int Q, bool PK = false, bool COH = false>
 __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigned char *smem_raw)
 {
     using CT = Chunk<T>;
@@ -136,7 +142,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                 const int c0 = __ldg(d.hub_chunk_start + v), c1 = __ldg(d.hub_chunk_start + v + 1);
                 for (int ch = c0; ch < c1; ++ch)
                     for (int c = 0; c < d.k; ++c)
-                        agg_s[c * RS + vi] = add_rn(agg_s[c * RS + vi], p[(size_t)ch * d.hub_pitch + c]);
+                        agg_s[c * RS + vi] = add_rn(agg_s[c * RS + vi], ld_tab<COH>(p + (size_t)ch * d.hub_pitch + c));
                 continue;
             }
             const int beg = __ldg(d.off + v), end = __ldg(d.off + v + 1);
@@ -172,7 +178,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                         const int q = lane_g + G * r;
                         acc[r] = CT::zero();
                         if (q < nchunk)
-                            for (int ch = c0; ch < c1; ++ch) CT::add(acc[r], p[(size_t)ch * prc + q]);
+                            for (int ch = c0; ch < c1; ++ch) CT::add(acc[r], ld_tab<COH>(p + (size_t)ch * prc + q));
                     }
                 } else {
 #pragma unroll
@@ -189,7 +195,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
 #pragma unroll
                             for (int r = 0; r < Q; ++r) {
                                 const int q = lane_g + G * r;
-                                x[u][r] = q < nchunk ? __ldg(auxc + (size_t)nb[u] * rowc + q) : CT::zero();
+                                x[u][r] = q < nchunk ? ld_tab<COH>(auxc + (size_t)nb[u] * rowc + q) : CT::zero();
                             }
 #pragma unroll
                         for (int u = 0; u < U; ++u)
@@ -201,7 +207,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
 #pragma unroll
                         for (int r = 0; r < Q; ++r) {
                             const int q = lane_g + G * r;
-                            if (q < nchunk) CT::add(acc[r], __ldg(row + q));
+                            if (q < nchunk) CT::add(acc[r], ld_tab<COH>(row + q));
                         }
                     }
                 }
@@ -224,7 +230,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
         const T *mainp = reinterpret_cast<const T *>(d.main);
         for (int vi = warp; vi < tv; vi += NW) {
             const T *row = mainp + (size_t)(v0 + vi) * d.main_pitch;
-            for (int c = lane; c < d.L_m; c += 32) main_s[c * RS + vi] = __ldg(row + c);
+            for (int c = lane; c < d.L_m; c += 32) main_s[c * RS + vi] = ld_tab<COH>(row + c);
         }
     }
     __syncthreads();
@@ -431,7 +437,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
 // in lane order: a fixed summation order.  A one-hot aux child counts colors.
 // Needs NT * 16 bytes of shared memory (the lane partials).
 // ---------------------------------------------------------------------------
-template <typename T, int NT>
+template <typename T, int NT, bool COH = false>
 __device__ __forceinline__ void hub_item(const HubArgs &h, int item, unsigned char *smem_raw)
 {
     using CT = Chunk<T>;
@@ -469,16 +475,16 @@ __device__ __forceinline__ void hub_item(const HubArgs &h, int item, unsigned ch
         if (r < R) {
             int e = beg + r;
             for (; e + 3 * R < end; e += 4 * R) {
-                const C x0 = __ldg(auxc + (size_t)__ldg(h.adj + e) * rowc + q);
-                const C x1 = __ldg(auxc + (size_t)__ldg(h.adj + e + R) * rowc + q);
-                const C x2 = __ldg(auxc + (size_t)__ldg(h.adj + e + 2 * R) * rowc + q);
-                const C x3 = __ldg(auxc + (size_t)__ldg(h.adj + e + 3 * R) * rowc + q);
+                const C x0 = ld_tab<COH>(auxc + (size_t)__ldg(h.adj + e) * rowc + q);
+                const C x1 = ld_tab<COH>(auxc + (size_t)__ldg(h.adj + e + R) * rowc + q);
+                const C x2 = ld_tab<COH>(auxc + (size_t)__ldg(h.adj + e + 2 * R) * rowc + q);
+                const C x3 = ld_tab<COH>(auxc + (size_t)__ldg(h.adj + e + 3 * R) * rowc + q);
                 CT::add(acc, x0);
                 CT::add(acc, x1);
                 CT::add(acc, x2);
                 CT::add(acc, x3);
             }
-            for (; e < end; e += R) CT::add(acc, __ldg(auxc + (size_t)__ldg(h.adj + e) * rowc + q));
+            for (; e < end; e += R) CT::add(acc, ld_tab<COH>(auxc + (size_t)__ldg(h.adj + e) * rowc + q));
             lanes[threadIdx.x] = acc;
         }
         __syncthreads();
