@@ -49,6 +49,9 @@ WORKLOADS = {
     "p3_rmat16_ef16": dict(scale=16, ef=16, template="p3", per_step=1, seed=7),
     "tree5_rmat20_ef6": dict(scale=20, ef=6, template="tree5", per_step=10, seed=7),
     "spider7_rmat21_ef8": dict(scale=21, ef=8, template="spider7", per_step=64, seed=7),
+    # the 12-vertex tree on R-MAT scale 18: the same kernels on a case small
+    # enough for full ncu captures (about 2 GB of tables, still above L2)
+    "tree12_rmat18_ef8": dict(scale=18, ef=8, template="tree12", per_step=1, seed=7),
 }
 DEFAULT_WORKLOAD = "tree12_rmat20_ef8"
 METRIC = "colorings/sec"
@@ -191,6 +194,7 @@ def main():
     ap.add_argument("--hub", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip timing the other form (plain vs batched)")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
@@ -243,6 +247,7 @@ def main():
     raws = []
     with Clocks(local) as clk:
         barrier()
+        torch.cuda.nvtx.range_push("timed")
         for s in range(args.steps):
             raw, st = sg.count(g, tmpl, B, seeds(args.warmup + s), batch=args.batch, hub_threshold=args.hub,
                                return_stats=True, profile=True)
@@ -255,10 +260,29 @@ def main():
             gather_bytes += st["fused_gather_bytes"]
             hub_ms += st["hub_ms"]
         barrier()
+        torch.cuda.nvtx.range_pop()
     clocks = clk.summary()
     total_ms = max_over_ranks(dev_ms)
     ms_per_step = total_ms / args.steps
     value = world * B * args.steps / (total_ms / 1000.0)
+
+    # the other form on the same colorings (plain <-> batched), for the batched-vs-plain ratio
+    forms = None
+    if not args.no_forms:
+        other = B if args.batch == 0 else 0
+        for s in range(min(args.warmup, 2)):
+            sg.count(g, tmpl, B, seeds(s), batch=other, hub_threshold=args.hub)
+        barrier()
+        other_ms = 0.0
+        for s in range(args.steps):
+            _, st = sg.count(g, tmpl, B, seeds(args.warmup + s), batch=other, hub_threshold=args.hub,
+                             return_stats=True)
+            other_ms += st["device_ms"]
+        barrier()
+        other_value = world * B * args.steps / (max_over_ranks(other_ms) / 1000.0)
+        plain_v, batched_v = (value, other_value) if args.batch == 0 else (other_value, value)
+        forms = {"plain": plain_v, "batched": batched_v, "batch": args.batch or B,
+                 "batched_over_plain": batched_v / plain_v, "unit": "colorings/s"}
 
     # end to end through the public API: pinned host CSC -> device graph -> count -> raw counts
     e2e = None
@@ -300,6 +324,8 @@ def main():
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if forms:
+        line["forms"] = forms
     if e2e:
         line["e2e"] = e2e
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

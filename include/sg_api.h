@@ -126,6 +126,8 @@ typedef struct {
     int32_t test_unsatisfiable_wait; /* test hook: in the batched form the first fused stage
                                also waits on a counter nothing increments, so the call
                                must end with SG_ERR_TIMEOUT */
+    int32_t no_blocked;     /* 1: no register-blocked eMA (every output computed by its
+                               own split loop); the two forms give identical values */
 } sg_count_opts;
 
 typedef struct {

@@ -317,6 +317,7 @@ sg_status sg_count(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw, s
     co.exact = o->exact ? 1 : 0;
     co.wait_limit_ms = o->wait_limit_ms;
     co.test_unsatisfiable_wait = o->test_unsatisfiable_wait;
+    co.blocked = o->no_blocked ? 0 : 1;
     sg::CountStats cs;
     sg_status st = from(sg::count(*g->g, p->p, co, raw, &cs));
     if (st) return st;

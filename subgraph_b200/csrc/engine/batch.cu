@@ -26,7 +26,7 @@ template <typename T>
 __device__ __forceinline__ void batch_fused(const StageDesc &d, int tile, unsigned char *smem)
 {
     constexpr int NT = kBatchThreads;
-    if (sizeof(T) == 4 && d.packed) {
+    if (sizeof(T) == 4 && d.packed == 1) {
         switch (d.gather_q) {
         case 1: fused_tile<T, NT, 1, true, true>(d, tile, smem); break;
         case 2: fused_tile<T, NT, 2, true, true>(d, tile, smem); break;

@@ -55,6 +55,7 @@ struct CountOptions {
     int32_t exact = 0;              // reference operation order everywhere: no hub chunks, no fused products
     int32_t wait_limit_ms = 0;      // batched queue: time a dependency wait may take (0 = 2000 ms)
     int32_t test_unsatisfiable_wait = 0;   // test hook: the first fused stage waits on a counter nothing sets
+    int32_t blocked = 1;            // register-blocked eMA where a stage has one (same values)
 };
 
 struct CountStats {

@@ -134,14 +134,21 @@ bool packed_ok(const StageDesc &d, bool fp64, int tv)
     return !fp64 && tv == 32 && !d.main_leaf && !d.is_root && !d.scaled && d.aoff && d.moff;
 }
 
+bool blocked_ok(const StageDesc &d, bool fp64, int tv, int nt)
+{
+    return !fp64 && (tv == 32 || tv == 16) && (nt == 256 || nt == 512) && d.blk && d.blk_shape > 0 &&
+           d.blk_nblocks > 0 && !d.main_leaf && !d.is_root && !d.scaled;
+}
+
 bool shape_fits(const StageDesc &d, bool fp64, int tv, int nt, int packed, size_t limit, size_t &bytes, int &oc)
 {
-    if (packed && !packed_ok(d, fp64, tv)) return false;
+    if (packed == 1 && !packed_ok(d, fp64, tv)) return false;
+    if (packed == 2 && !blocked_ok(d, fp64, tv, nt)) return false;
     const int La_rows = d.aux_leaf ? d.k : d.L_a;
     const int Lm_rows = d.main_leaf ? 0 : d.L_m;
-    oc = (d.is_root || d.main_leaf) ? 0 : std::min(d.L_s, nt >= 1024 ? 256 : 128);
+    oc = (d.is_root || d.main_leaf) ? 0 : (packed == 2 ? d.L_s : std::min(d.L_s, nt >= 1024 ? 256 : 128));
     bytes = fp64 ? tile_smem_bytes<double>(La_rows, Lm_rows, oc, tv, false)
-                 : tile_smem_bytes<float>(La_rows, Lm_rows, oc, tv, packed != 0);
+                 : tile_smem_bytes<float>(La_rows, Lm_rows, oc, tv, packed == 1);
     if (bytes > limit) return false;
     if (!d.aux_leaf) {
         const int CH = fp64 ? 2 : 4;
@@ -172,8 +179,14 @@ std::vector<TileShape> candidate_shapes(const StageDesc &d, bool fp64)
     const bool heavy = !d.main_leaf && !d.is_root && (int64_t)d.S * d.L_s >= 512;
     if (d.aux_leaf) all = {{256, 256, 0}, {64, 256, 0}, {32, 256, 0}, {128, 512, 0}};
     else if (heavy)
-        all = {{32, 1024, 1}, {32, 512, 1}, {32, 256, 1}, {32, 1024, 0}, {32, 512, 0}, {32, 256, 0}, {16, 256, 0}};
+        all = {{32, 1024, 1}, {32, 512, 1}, {32, 256, 1}, {32, 1024, 0}, {32, 512, 0}, {32, 256, 0},
+               {16, 256, 0}, {16, 512, 0}, {16, 1024, 0}};
+    else if (!d.aux_leaf && d.L_a >= 128)   // wide gathers: more threads per CTA for loads in flight
+        all = {{8, 256, 0}, {16, 256, 0}, {32, 256, 0}, {32, 512, 0}, {8, 512, 0}, {16, 512, 0}, {16, 1024, 0}};
     else all = {{8, 256, 0}, {16, 256, 0}, {32, 256, 0}, {32, 512, 0}};
+    if (d.blk_shape > 0)   // register-blocked eMA
+        for (TileShape t : {TileShape{32, 256, 2}, TileShape{32, 512, 2}, TileShape{16, 256, 2}, TileShape{16, 512, 2}})
+            all.push_back(t);
     for (auto &c : all) {
         size_t bytes;
         int oc;
@@ -191,7 +204,10 @@ bool plan_fused(StageDesc &d, bool fp64, int sm_count, FusedConfig &cfg)
     const size_t limits[3] = {56 * 1024, 113 * 1024, 227 * 1024};
     bool ok = false;
     d.packed = 0;
-    if (heavy) {
+    // the register-blocked eMA when the stage has one (its sums are those of the per-output loop)
+    for (TileShape t : {TileShape{32, 256, 2}, TileShape{16, 256, 2}, TileShape{32, 512, 2}, TileShape{16, 512, 2}})
+        if (!ok && d.blk_shape > 0) ok = set_shape(d, fp64, t);
+    if (heavy && !ok) {
         // 32-vertex tiles keep the eMA free of bank conflicts; a wide tile gets 512 threads
         const int pk = packed_ok(d, fp64, 32) ? 1 : 0;
         size_t bytes;
@@ -225,7 +241,7 @@ static void launch_fused_q(const StageDesc &d, const FusedConfig &cfg, cudaStrea
         const int grid = std::max(1, std::min(d.ntiles, cfg.grid * per_sm));
         kern<<<grid, NT, cfg.smem, st>>>(d);
     };
-    if (d.packed) {
+    if (d.packed == 1) {
         switch (d.gather_q) {
         case 1: go(k_fused<float, NT, 1, true>); break;
         case 2: go(k_fused<float, NT, 2, true>); break;
@@ -243,6 +259,10 @@ static void launch_fused_q(const StageDesc &d, const FusedConfig &cfg, cudaStrea
 void launch_fused(const StageDesc &d, bool fp64, const FusedConfig &cfg, cudaStream_t st)
 {
     if (d.V == 0) return;
+    if (!fp64 && d.packed == 2) {
+        launch_fused_blk(d, cfg, st);
+        return;
+    }
     if (fp64) {
         if (d.nthreads == 1024) launch_fused_q<double, 1024>(d, cfg, st);
         else if (d.nthreads == 512) launch_fused_q<double, 512>(d, cfg, st);

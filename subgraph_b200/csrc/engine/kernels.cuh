@@ -48,7 +48,7 @@ bool plan_fused(StageDesc &d, bool fp64, int sm_count, FusedConfig &cfg);
 struct TileShape {
     int tile_v;      // vertices per tile
     int threads;     // CTA size
-    int packed;      // packed FP32x2 eMA (32-vertex tiles)
+    int packed;      // eMA form: 0 per-output loop, 1 packed FP32x2 (32-vertex tiles), 2 register-blocked
 };
 // Sets an explicit shape (the autotuner's candidates); false when it does not fit.
 bool set_shape(StageDesc &d, bool fp64, const TileShape &shape);
@@ -57,6 +57,8 @@ std::vector<TileShape> candidate_shapes(const StageDesc &d, bool fp64);
 void launch_fused(const StageDesc &d, bool fp64, const FusedConfig &cfg, cudaStream_t st);
 void launch_hub(const HubArgs &h, bool fp64, int sm_count, cudaStream_t st);
 
+// K2 with the register-blocked eMA (StageDesc::packed == 2)
+void launch_fused_blk(const StageDesc &d, const FusedConfig &cfg, cudaStream_t st);
 void launch_root_reduce(const double *partial, int32_t n, double scale, double *out, cudaStream_t st);
 
 // the batched form (batch.cu)

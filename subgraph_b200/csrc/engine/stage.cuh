@@ -41,11 +41,16 @@ struct StageDesc {
     void *out;
     const uint32_t *split;             // [S][split_stride] (main col | aux col << 16) per (split, output column)
     int32_t split_stride;              // L_s rounded up to a multiple of 4
-    // packed eMA (FP32, 32-vertex tiles, two vertices per lane): shared rows of
-    // kPackedRow floats and the split table as byte offsets into shared memory
+    // eMA form: 0 per-output loop; 1 packed (FP32, 32-vertex tiles, two
+    // vertices per lane: shared rows of kPackedRow floats and the split table
+    // as byte offsets into shared memory); 2 register-blocked (FP32, the
+    // outputs grouped by (|s|+1)-color supersets, blk_sched.hpp)
     int32_t packed;
     const uint32_t *aoff;              // [S][split_stride] aggregate row byte offset
     const uint32_t *moff;              // [S][split_stride] main row byte offset
+    const int32_t *blk;                // [blk_nblocks][row] held / streamed / output columns per block
+    int32_t blk_shape;                 // blk::shape_id of (|s|, |main|), 0 = no blocked form
+    int32_t blk_nblocks;
     const int16_t *rem;                // [L_s][k] main-leaf: aux column of set\{c}, or -1
     const uint8_t *color;              // [V] internal order
     const int32_t *off;                // [V+1]

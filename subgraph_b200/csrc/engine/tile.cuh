@@ -10,6 +10,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "blk_ema.cuh"
 #include "stage.cuh"
 
 namespace sg {
@@ -61,6 +62,27 @@ template <bool COH, typename P> __device__ __forceinline__ P ld_tab(const P *p) 
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 
+// Quotient by a tile-uniform divisor d for 0 <= i < n: multiply-high by
+// m = floor((2^32-1)/d) + 1, exact while n*d < 2^32 (the error term i*(m*d -
+// 2^32)/2^32 stays below 1/d); otherwise the plain division.
+struct FastDiv {
+    uint32_t m;
+    int d;
+    bool ok;
+};
+__device__ __forceinline__ FastDiv fast_div(int d, int n)
+{
+    FastDiv f;
+    f.d = d;
+    f.ok = d > 1 && (uint64_t)n * (uint64_t)d < (1ull << 32);
+    f.m = f.ok ? 0xffffffffu / (uint32_t)d + 1u : 0u;
+    return f;
+}
+__device__ __forceinline__ int fdiv(const FastDiv &f, int i)
+{
+    return f.ok ? (int)__umulhi((uint32_t)i, f.m) : i / f.d;
+}
+
 // Row stride (floats) of the aggregate and main rows in the packed layout: 32
 // vertices plus 2 so that the 16 float2 of a half-warp cover all 32 banks.
 constexpr int kPackedRow = 34;
@@ -107,7 +129,7 @@ __device__ __forceinline__ unsigned long long add2_rn(unsigned long long a, unsi
 //      per vertex, reduced over the tile in a fixed order.
 // The aggregate never leaves the chip.
 // ---------------------------------------------------------------------------
-template <typename T, int NT, int Q, bool PK = false, bool COH = false>
+template <typename T, int NT, int Q, bool PK = false, bool COH = false, bool BLK = false>
 __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigned char *smem_raw)
 {
     using CT = Chunk<T>;
@@ -146,17 +168,18 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                 continue;
             }
             const int beg = __ldg(d.off + v), end = __ldg(d.off + v + 1);
-            int e = beg;
-            for (; e + 8 <= end; e += 8) {
+            // batches of 8 neighbours, the last one predicated: every batch
+            // has its loads in flight together
+            for (int e = beg; e < end; e += 8) {
                 int nb[8], cl[8];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) nb[u] = __ldg(d.adj + e + u);
+                for (int u = 0; u < 8; ++u) nb[u] = e + u < end ? __ldg(d.adj + e + u) : -1;
 #pragma unroll
-                for (int u = 0; u < 8; ++u) cl[u] = __ldg(d.color + nb[u]);
+                for (int u = 0; u < 8; ++u) cl[u] = nb[u] >= 0 ? (int)__ldg(d.color + nb[u]) : -1;
 #pragma unroll
-                for (int u = 0; u < 8; ++u) agg_s[cl[u] * RS + vi] += T(1);
+                for (int u = 0; u < 8; ++u)
+                    if (cl[u] >= 0) agg_s[cl[u] * RS + vi] += T(1);
             }
-            for (; e < end; ++e) agg_s[__ldg(d.color + __ldg(d.adj + e)) * RS + vi] += T(1);
         }
     } else {
         const int G = d.gather_group;
@@ -184,31 +207,26 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
 #pragma unroll
                     for (int r = 0; r < Q; ++r) acc[r] = CT::zero();
                     const int beg = __ldg(d.off + v), end = __ldg(d.off + v + 1);
-                    int e = beg;
-                    for (; e + U <= end; e += U) {
+                    // batches of U neighbours with all their row loads in flight;
+                    // the last batch is predicated and its idle slots add +0,
+                    // which leaves every (non-negative) sum bit-identical
+                    for (int e = beg; e < end; e += U) {
                         int nb[U];
 #pragma unroll
-                        for (int u = 0; u < U; ++u) nb[u] = __ldg(d.adj + e + u);
+                        for (int u = 0; u < U; ++u) nb[u] = e + u < end ? __ldg(d.adj + e + u) : -1;
                         C x[U][Q];
 #pragma unroll
                         for (int u = 0; u < U; ++u)
 #pragma unroll
                             for (int r = 0; r < Q; ++r) {
                                 const int q = lane_g + G * r;
-                                x[u][r] = q < nchunk ? ld_tab<COH>(auxc + (size_t)nb[u] * rowc + q) : CT::zero();
+                                x[u][r] = (q < nchunk && nb[u] >= 0) ? ld_tab<COH>(auxc + (size_t)nb[u] * rowc + q)
+                                                                     : CT::zero();
                             }
 #pragma unroll
                         for (int u = 0; u < U; ++u)
 #pragma unroll
                             for (int r = 0; r < Q; ++r) CT::add(acc[r], x[u][r]);
-                    }
-                    for (; e < end; ++e) {
-                        const C *row = auxc + (size_t)__ldg(d.adj + e) * rowc;
-#pragma unroll
-                        for (int r = 0; r < Q; ++r) {
-                            const int q = lane_g + G * r;
-                            if (q < nchunk) CT::add(acc[r], ld_tab<COH>(row + q));
-                        }
                     }
                 }
 #pragma unroll
@@ -279,15 +297,34 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
         // one-hot main: out[o] = agg[set(o) \ {color}] when color is in set(o)
         T *outp = reinterpret_cast<T *>(d.out);
         const int P = d.out_pitch;
+        // the tile's rows are contiguous: one flat, coalesced pass over them
+        const FastDiv fd = fast_div(P, tv * P);
+        T *tile_out = outp + (size_t)v0 * P;
         for (int idx = tid; idx < tv * P; idx += NT) {
-            const int vi = idx / P, o = idx - vi * P;
+            const int vi = fdiv(fd, idx), o = idx - vi * P;
             T val = T(0);
             if (o < d.L_s) {
                 const int cv = __ldg(d.color + v0 + vi);
                 const int r = __ldg(d.rem + o * d.k + cv);
                 if (r >= 0) val = leaf_value(agg_s[r * RS + vi], scaled);
             }
-            outp[(size_t)(v0 + vi) * P + o] = val;
+            tile_out[idx] = val;
+        }
+    } else if (BLK && d.packed == 2) {
+        // register-blocked eMA over all output columns at once (blk_ema.cuh),
+        // then the rows of the tile written out contiguously
+        if constexpr (BLK && sizeof(T) == 4 && !PK) {
+            T *outp = reinterpret_cast<T *>(d.out);
+            const int P = d.out_pitch;
+            blk::ema_blocked(d, agg_s, main_s, out_s, RS, TVP, TV, warp, NW, lane);
+            __syncthreads();
+            const FastDiv fd = fast_div(P, tv * P);
+            T *tile_out = outp + (size_t)v0 * P;
+            for (int idx = tid; idx < tv * P; idx += NT) {
+                const int vj = fdiv(fd, idx), t = idx - vj * P;
+                tile_out[idx] = t < d.L_s ? out_s[t * TVP + vj] : T(0);
+            }
+            __syncthreads();
         }
     } else if (PK) {
         // packed eMA: lane = pair of vertices (2p, 2p+1) x a group of 4 output
@@ -359,8 +396,9 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
             }
             __syncthreads();
             const int ow = (o0 + oc == d.L_s) ? P - o0 : oc;
+            const FastDiv fd = fast_div(ow, tv * ow);
             for (int idx = tid; idx < tv * ow; idx += NT) {
-                const int vj = idx / ow, t = idx - vj * ow;
+                const int vj = fdiv(fd, idx), t = idx - vj * ow;
                 outp[(size_t)(v0 + vj) * P + o0 + t] = t < oc ? out_s[t * TVP + vj] : T(0);
             }
             __syncthreads();
@@ -420,8 +458,9 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
             }
             __syncthreads();
             const int ow = (o0 + oc == d.L_s) ? P - o0 : oc;   // the last chunk zero-fills the row padding
+            const FastDiv fd = fast_div(ow, tv * ow);
             for (int idx = tid; idx < tv * ow; idx += NT) {
-                const int vj = idx / ow, t = idx - vj * ow;
+                const int vj = fdiv(fd, idx), t = idx - vj * ow;
                 outp[(size_t)(v0 + vj) * P + o0 + t] = t < oc ? out_s[t * TVP + vj] : T(0);
             }
             __syncthreads();
