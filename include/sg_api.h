@@ -110,7 +110,7 @@ typedef struct {
     int32_t n_colorings;    /* iterations (CountMat::initialization itr_num) */
     uint32_t seed_base;     /* coloring c uses srand(seed_base + c) */
     int32_t mode;           /* SG_MODE_* */
-    int32_t batch;          /* > 0: colorings per persistent launch; 0: plain */
+    int32_t batch;          /* > 0: colorings per batch (batched form); 0: plain */
     int32_t hub_threshold;  /* degree above which aggregation is chunked; 0 = never
                                (exact reference arithmetic for every vertex) */
     int32_t profile;        /* != 0: time every fused launch with CUDA events */
@@ -128,6 +128,9 @@ typedef struct {
                                must end with SG_ERR_TIMEOUT */
     int32_t no_blocked;     /* 1: no register-blocked eMA (every output computed by its
                                own split loop); the two forms give identical values */
+    int32_t persistent;     /* batched form: 1 = one persistent work-queue launch per batch
+                               (colorings in separate table slots); 0 = interleaved groups
+                               (the batch's colorings share table rows and neighbour passes) */
 } sg_count_opts;
 
 typedef struct {

@@ -48,7 +48,8 @@ class CountOpts(ctypes.Structure):
     _fields_ = [("n_colorings", ctypes.c_int32), ("seed_base", ctypes.c_uint32), ("mode", ctypes.c_int32),
                 ("batch", ctypes.c_int32), ("hub_threshold", ctypes.c_int32), ("profile", ctypes.c_int32),
                 ("no_autotune", ctypes.c_int32), ("exact", ctypes.c_int32), ("wait_limit_ms", ctypes.c_int32),
-                ("test_unsatisfiable_wait", ctypes.c_int32), ("no_blocked", ctypes.c_int32)]
+                ("test_unsatisfiable_wait", ctypes.c_int32), ("no_blocked", ctypes.c_int32),
+                ("persistent", ctypes.c_int32)]
 
 
 class CountStats(ctypes.Structure):

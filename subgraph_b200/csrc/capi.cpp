@@ -318,6 +318,7 @@ sg_status sg_count(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw, s
     co.wait_limit_ms = o->wait_limit_ms;
     co.test_unsatisfiable_wait = o->test_unsatisfiable_wait;
     co.blocked = o->no_blocked ? 0 : 1;
+    co.persistent = o->persistent;
     sg::CountStats cs;
     sg_status st = from(sg::count(*g->g, p->p, co, raw, &cs));
     if (st) return st;

@@ -526,6 +526,7 @@ struct RunCtx {
     bool profile = false;
     bool autotune = false;
     bool blocked = true;     // register-blocked eMA allowed
+    int lay = 1;             // colorings interleaved per table row (grouped batched form)
     bool exact = false;      // no fused products (packed eMA), no hub chunks
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> fused_ev, hub_ev;
     double fused_alg_bytes = 0, fused_gather_bytes = 0;
@@ -567,11 +568,12 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
     SG_CKS(growT(&w.raw, &w.raw_bytes, 8 * (size_t)std::max(ncolorings_total, 1), g.stream));
     SG_CKS(growT(&w.windows, &w.windows_bytes, 4 * 31 * (size_t)std::max(ncolorings_total, 1), g.stream));
     if (c.hubs.count > 0) {
-        int32_t maxp = round_up(c.p.k, 4);
+        // a partial row holds the aux columns (or colour counts) of up to c.lay colorings
+        int32_t maxp = round_up(c.lay * c.p.k, 4);
         for (int s : c.p.process_order) {
             const SubTemplate &st = c.p.subs[s];
             const SubTemplate &a = c.p.subs[st.aux];
-            if (a.size > 1) maxp = std::max<int32_t>(maxp, c.p.table_pitch[st.aux]);
+            if (a.size > 1) maxp = std::max<int32_t>(maxp, c.lay * c.p.table_pitch[st.aux]);
         }
         c.hub_pitch = maxp;
         SG_CKS(grow(&w.hub_partial, &w.hub_partial_bytes, (size_t)c.hubs.total_chunks * maxp * c.es, g.stream));
@@ -583,14 +585,18 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
     return Status::ok();
 }
 
+// Table of sub `sub` in color slot `slot`; with c.lay colorings interleaved
+// the table is [V][lay][pitch] at lay times the per-coloring offset.
 void *table_ptr(RunCtx &c, int slot, int sub)
 {
-    return (char *)c.gs.ws.arena + c.arena_per_coloring * slot + (size_t)c.p.table_offset[sub] * c.g.V * c.es;
+    return (char *)c.gs.ws.arena + c.arena_per_coloring * slot +
+           (size_t)c.lay * c.p.table_offset[sub] * c.g.V * c.es;
 }
 
-// The descriptor of one sub-template step of the coloring in color slot `slot`
-// (shape fields left for plan_fused / set_shape).
-StageDesc make_stage(RunCtx &c, int slot, int s, double *root_vertex)
+// The descriptor of one sub-template step of the coloring in color slot `slot`,
+// or of colorings [b0, b0 + nb) of an interleaved group (c.lay > 1, slot 0);
+// shape fields are left for plan_fused / set_shape.
+StageDesc make_stage(RunCtx &c, int slot, int s, double *root_vertex, int b0 = 0, int nb = 1)
 {
     const Plan &p = c.p;
     const SubTemplate &sub = p.subs[s];
@@ -609,12 +615,25 @@ StageDesc make_stage(RunCtx &c, int slot, int s, double *root_vertex)
     d.is_root = s == 0;
     d.scaled = (c.mode == kModeReference && s == p.scaled_sub && s != 0) ? 1 : 0;
     d.root_float = c.mode == kModeOriginal;
-    d.out_pitch = s == 0 ? 0 : p.table_pitch[s];
-    d.main_pitch = d.main_leaf ? 0 : p.table_pitch[sub.main];
-    d.aux_pitch = d.aux_leaf ? 0 : p.table_pitch[sub.aux];
-    d.main = d.main_leaf ? nullptr : table_ptr(c, slot, sub.main);
-    d.aux = d.aux_leaf ? nullptr : table_ptr(c, slot, sub.aux);
-    d.out = s == 0 ? nullptr : table_ptr(c, slot, s);
+    const int L = c.lay;
+    const int ps = s == 0 ? 0 : p.table_pitch[s];
+    const int pm = d.main_leaf ? 0 : p.table_pitch[sub.main];
+    const int pa = d.aux_leaf ? 0 : p.table_pitch[sub.aux];
+    d.nb = nb;
+    d.cstride = L;
+    d.out_pitch = L * ps;
+    d.main_pitch = L * pm;
+    d.aux_pitch = L * pa;
+    d.aux_cols = d.aux_leaf ? nb * p.k : (nb == 1 ? a.L : nb * pa);   // one-hot: the histogram's columns
+    d.a_cstride = d.aux_leaf ? p.k : pa;
+    d.main_cols = nb == 1 ? m.L : nb * pm;
+    d.m_cstride = pm;
+    d.out_w = nb * ps;
+    d.s_cstride = ps;
+    d.rp_stride = g.V / 8 + 2;
+    d.main = d.main_leaf ? nullptr : (char *)table_ptr(c, slot, sub.main) + (size_t)b0 * pm * c.es;
+    d.aux = d.aux_leaf ? nullptr : (char *)table_ptr(c, slot, sub.aux) + (size_t)b0 * pa * c.es;
+    d.out = s == 0 ? nullptr : (char *)table_ptr(c, slot, s) + (size_t)b0 * ps * c.es;
     d.split = c.tab->split[s];
     d.split_stride = (sub.L + 3) / 4 * 4;
     d.rem = c.tab->rem[s];
@@ -625,11 +644,11 @@ StageDesc make_stage(RunCtx &c, int slot, int s, double *root_vertex)
     d.blk = (c.fp64 || !c.blocked) ? nullptr : c.tab->blk[s];
     d.blk_shape = d.blk ? c.tab->blk_shape[s] : 0;
     d.blk_nblocks = d.blk ? c.tab->blk_nblocks[s] : 0;
-    d.color = w.colors + (size_t)slot * g.V;
+    d.color = w.colors + (size_t)slot * g.V + b0;
     d.off = g.d_off;
     d.adj = g.d_adj;
-    d.root_partial = w.partial + (size_t)slot * (g.V / 8 + 2);
-    d.root_vertex = root_vertex;
+    d.root_partial = w.partial + (size_t)(slot + b0) * (g.V / 8 + 2);
+    d.root_vertex = nb == 1 ? root_vertex : nullptr;
     return d;
 }
 
@@ -641,10 +660,12 @@ HubArgs make_hub(RunCtx &c, StageDesc &d, void *partial)
     HubArgs h{};
     h.hub_count = c.hubs.count;
     h.chunk = c.hubs.chunk;
-    h.L_a = d.L_a;
+    h.L_a = d.aux_cols;
     h.aux_pitch = d.aux_pitch;
     h.row_pitch = c.hub_pitch;
     h.k_leaf = d.aux_leaf ? c.p.k : 0;
+    h.nb = d.nb;
+    h.cstride = d.cstride;
     h.color = d.color;
     h.total_chunks = c.hubs.total_chunks;
     h.chunk_start = c.gs.ws.chunk_start;
@@ -660,10 +681,10 @@ HubArgs make_hub(RunCtx &c, StageDesc &d, void *partial)
 }
 
 // One sub-template step of the coloring in color slot `slot`.
-Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t st)
+Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t st, int b0 = 0, int nb = 1)
 {
     DeviceGraph &g = c.g;
-    StageDesc d = make_stage(c, slot, s, root_vertex);
+    StageDesc d = make_stage(c, slot, s, root_vertex, b0, nb);
     if (c.hubs.count > 0) {
         HubArgs h = make_hub(c, d, c.gs.ws.hub_partial);
         if (c.profile) {
@@ -681,8 +702,8 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
         // autotuner: the first time a stage shape runs on this graph, time every
         // (tile vertices, CTA threads) candidate on the real inputs; all of them
         // compute the same values, so the trial launches only cost time
-        const std::string key =
-            graph_sig(g) + shape_key(d, c.fp64, c.hubs.count) + (d.aoff ? "/pk" : "/ex") + (d.blk ? "/bk" : "");
+        const std::string key = graph_sig(g) + shape_key(d, c.fp64, c.hubs.count) + (d.aoff ? "/pk" : "/ex") +
+                                (d.blk ? "/bk" : "") + "/n" + std::to_string(d.nb) + "/l" + std::to_string(c.lay);
         TileShape pick{d.tile_v, d.nthreads, d.packed};
         bool have = false;
         {
@@ -738,10 +759,10 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
         // compulsory traffic: main and aux tables read once (a one-hot child is read
         // as the colors array: one element per vertex), the output written once and
         // the adjacency read once (offsets + neighbour ids)
-        const double V = (double)g.V;
+        const double V = (double)g.V, nb = (double)d.nb;
         const double lm = d.main_leaf ? 1.0 : (double)d.L_m, la = d.aux_leaf ? 1.0 : (double)d.L_a;
-        c.fused_alg_bytes += (double)c.es * V * (lm + la + (s ? (double)d.L_s : 0.0)) + 4.0 * (V + 1 + (double)g.nnz);
-        c.fused_gather_bytes += (double)c.es * (double)g.nnz * (d.aux_leaf ? 0.25 : (double)d.L_a);
+        c.fused_alg_bytes += nb * (double)c.es * V * (lm + la + (s ? (double)d.L_s : 0.0)) + 4.0 * (V + 1 + (double)g.nnz);
+        c.fused_gather_bytes += nb * (double)c.es * (double)g.nnz * (d.aux_leaf ? 0.25 : (double)d.L_a);
     }
     c.launches += 1;
     if (s == 0) c.root_tiles = d.ntiles;
@@ -760,7 +781,8 @@ Status launch_colors(RunCtx &c, int slot0, int first_coloring, int n, cudaStream
     a.window = c.gs.ws.windows + 31 * (size_t)first_coloring;
     a.perm = c.g.d_perm;
     a.color = c.gs.ws.colors + (size_t)slot0 * c.g.V;
-    a.color_stride = c.g.V;
+    a.color_stride = c.lay == 1 ? c.g.V : 1;   // [n][V], or interleaved [V][lay]
+    a.vertex_stride = c.lay;
     launch_color(a, n, st);
     c.launches += 1;
     SG_CK(cudaGetLastError());
@@ -1010,6 +1032,124 @@ Status count_batched(RunCtx &c, const CountOptions &o, double *raw, CountStats *
 
 }  // namespace
 
+// Interleaved groups: colorings per launch of each stage.  Every candidate
+// nb in (lay, lay/2, ..., 1) whose tile fits shared memory is timed over a
+// whole stage pass (all its launches, each with tuned tile shapes) once per
+// graph, stage shape and group size; the fastest is kept.  Passes recompute
+// the same table from the same inputs (an output never overlaps its inputs
+// in the arena), so trial passes are harmless.
+std::map<std::string, int> g_group_nb;
+
+Status run_stage_group(RunCtx &c, int s, cudaStream_t st)
+{
+    const int L = c.lay;
+    auto pass = [&](int nb) -> Status {
+        for (int b0 = 0; b0 < L; b0 += nb) SG_CKS(run_stage(c, 0, s, nullptr, st, b0, std::min(nb, L - b0)));
+        return Status::ok();
+    };
+    if (L == 1) return pass(1);
+    StageDesc d1 = make_stage(c, 0, s, nullptr, 0, 1);
+    const std::string key = graph_sig(c.g) + shape_key(d1, c.fp64, c.hubs.count) + "/lay" + std::to_string(L) +
+                            (c.exact ? "/ex" : "") + (c.blocked ? "/bk" : "");
+    int nb = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_state_mu);
+        auto it = g_group_nb.find(key);
+        if (it != g_group_nb.end()) nb = it->second;
+    }
+    if (nb == 0) {
+        std::vector<int> cands;
+        for (int n = L;; n = (n + 1) / 2) {
+            StageDesc dn = make_stage(c, 0, s, nullptr, 0, n);
+            FusedConfig cfg;
+            if (plan_fused(dn, c.fp64, c.g.sm_count, cfg)) cands.push_back(n);
+            if (n == 1) break;
+        }
+        if (cands.empty()) return Status{6, "sub-template " + std::to_string(s) + " needs more shared memory than a CTA has"};
+        nb = cands.front();
+        if (c.autotune && cands.size() > 1) {
+            cudaEvent_t e0, e1;
+            SG_CK(cudaEventCreate(&e0));
+            SG_CK(cudaEventCreate(&e1));
+            float best = 1e30f;
+            for (int n : cands) {
+                SG_CKS(pass(n));   // tunes the tile shapes of this nb
+                SG_CK(cudaEventRecord(e0, st));
+                SG_CKS(pass(n));
+                SG_CK(cudaEventRecord(e1, st));
+                SG_CK(cudaEventSynchronize(e1));
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (std::getenv("SG_TUNE_LOG"))
+                    std::fprintf(stderr, "[sg tune] sub %d group %d colorings per launch %d: %.3f ms\n", s, L, n, ms);
+                if (ms < best) { best = ms; nb = n; }
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+        }
+        std::lock_guard<std::mutex> lk(g_state_mu);
+        g_group_nb[key] = nb;
+    }
+    return pass(nb);
+}
+
+// Grouped batched form: `batch` colorings interleaved per table row ([V][B]
+// colors, [V][B][pitch] tables), every stage launched for several colorings
+// at once so one pass over a vertex's neighbour list serves all of them.
+// The group size is admitted by free device memory.
+Status count_grouped(RunCtx &c, const CountOptions &o, double *raw, CountStats *stats)
+{
+    DeviceGraph &g = c.g;
+    const Plan &p = c.p;
+    cudaStream_t st = g.stream;
+    int B = std::max(1, std::min(o.batch, o.n_colorings));
+    {
+        size_t free_b = 0, total_b = 0;
+        SG_CK(cudaMemGetInfo(&free_b, &total_b));
+        const size_t V = (size_t)g.V;
+        const size_t per = (size_t)p.arena_units * V * c.es + V + 8 * (V / 8 + 2);
+        const size_t have = c.gs.ws.arena_bytes + c.gs.ws.colors_bytes + c.gs.ws.partial_bytes;
+        while (B > 1 && per * (size_t)B > (size_t)((double)(free_b + have) * 0.85)) B = (B + 1) / 2;
+    }
+    c.lay = B;
+    SG_CKS(prepare(c, B, o.n_colorings));
+    SG_CKS(upload_windows(c, o.seed_base, o.n_colorings));
+    cudaEvent_t e0, e1;
+    SG_CK(cudaEventCreate(&e0));
+    SG_CK(cudaEventCreate(&e1));
+    SG_CK(cudaEventRecord(e0, st));
+    const double scale = o.mode == kModeReference ? 1.0e12 : 1.0;
+    for (int g0 = 0; g0 < o.n_colorings; g0 += B) {
+        c.lay = std::min(B, o.n_colorings - g0);
+        SG_CKS(launch_colors(c, 0, g0, c.lay, st));
+        for (int s : p.process_order) SG_CKS(run_stage_group(c, s, st));
+        launch_root_reduce_slots(c.gs.ws.partial, (int64_t)(g.V / 8 + 2), c.root_tiles, scale, c.gs.ws.raw + g0, c.lay,
+                                 st);
+        c.launches += 1;
+        SG_CK(cudaGetLastError());
+    }
+    SG_CK(cudaEventRecord(e1, st));
+    SG_CK(cudaMemcpyAsync(raw, c.gs.ws.raw, sizeof(double) * o.n_colorings, cudaMemcpyDeviceToHost, st));
+    SG_CK(cudaStreamSynchronize(st));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (stats) {
+        stats->device_ms = ms;
+        stats->kernel_launches = c.launches;
+        stats->table_bytes = (int64_t)(c.arena_per_coloring * B);
+        stats->fused_launches = (int64_t)c.fused_ev.size();
+        stats->fused_ms = ev_sum(c.fused_ev);
+        stats->hub_ms = ev_sum(c.hub_ev);
+        stats->fused_alg_bytes = c.fused_alg_bytes;
+        stats->fused_gather_bytes = c.fused_gather_bytes;
+    }
+    ev_sum(c.fused_ev);
+    ev_sum(c.hub_ev);
+    return Status::ok();
+}
+
 Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, CountStats *stats)
 {
     if (o.n_colorings < 1) return Status{1, "n_colorings must be >= 1"};
@@ -1024,7 +1164,7 @@ Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, 
     c.profile = o.profile != 0;
     c.autotune = o.autotune != 0;
     c.blocked = o.blocked != 0;
-    if (o.batch > 0) return count_batched(c, o, raw, stats);
+    if (o.batch > 0) return o.persistent ? count_batched(c, o, raw, stats) : count_grouped(c, o, raw, stats);
     const int slots = 1;
     SG_CKS(prepare(c, slots, o.n_colorings));
     SG_CKS(upload_windows(c, o.seed_base, o.n_colorings));

@@ -48,7 +48,8 @@ struct CountOptions {
     int32_t n_colorings = 1;
     uint32_t seed_base = 0;
     int32_t mode = kModeReference;
-    int32_t batch = 0;              // > 0: colorings per persistent launch; 0: plain
+    int32_t batch = 0;              // > 0: colorings per batch (interleaved group); 0: plain
+    int32_t persistent = 0;         // batched: one persistent work-queue launch per batch instead
     int32_t hub_threshold = 1024;   // degree above which a vertex is aggregated in chunks; 0 = never
     int32_t profile = 0;            // time every fused launch with CUDA events
     int32_t autotune = 1;           // time the tile-shape candidates of new stage shapes once per graph

@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(kColorBlock) k_color(ColorArgs a)
 #pragma unroll
         for (int i = 0; i < 31; ++i) s += __ldg(a.coef + i * kColorBlock + threadIdx.x) * W[i];
         const int r = (int)(s >> 1);
-        a.color[col * a.color_stride + a.perm[v]] = (uint8_t)(r % a.k);
+        a.color[col * a.color_stride + (int64_t)a.perm[v] * a.vertex_stride] = (uint8_t)(r % a.k);
     }
 }
 
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(NT) k_hub(HubArgs h)
 void choose_gather(StageDesc &d, bool fp64)
 {
     const int CH = fp64 ? 2 : 4;
-    const int nchunk = (d.L_a + CH - 1) / CH;
+    const int nchunk = (d.aux_cols + CH - 1) / CH;
     const int NT = d.nthreads;
     int bestQ = 4, bestG = (nchunk + 3) / 4, bestActive = -1;
     for (int Q : {1, 2, 4}) {
@@ -131,12 +131,12 @@ void choose_gather(StageDesc &d, bool fp64)
 
 bool packed_ok(const StageDesc &d, bool fp64, int tv)
 {
-    return !fp64 && tv == 32 && !d.main_leaf && !d.is_root && !d.scaled && d.aoff && d.moff;
+    return !fp64 && tv == 32 && d.nb == 1 && !d.main_leaf && !d.is_root && !d.scaled && d.aoff && d.moff;
 }
 
 bool blocked_ok(const StageDesc &d, bool fp64, int tv, int nt)
 {
-    return !fp64 && (tv == 32 || tv == 16) && (nt == 256 || nt == 512) && d.blk && d.blk_shape > 0 &&
+    return !fp64 && (tv == 32 || tv == 16) && (nt == 256 || nt == 512) && d.nb == 1 && d.blk && d.blk_shape > 0 &&
            d.blk_nblocks > 0 && !d.main_leaf && !d.is_root && !d.scaled;
 }
 
@@ -144,15 +144,18 @@ bool shape_fits(const StageDesc &d, bool fp64, int tv, int nt, int packed, size_
 {
     if (packed == 1 && !packed_ok(d, fp64, tv)) return false;
     if (packed == 2 && !blocked_ok(d, fp64, tv, nt)) return false;
-    const int La_rows = d.aux_leaf ? d.k : d.L_a;
-    const int Lm_rows = d.main_leaf ? 0 : d.L_m;
-    oc = (d.is_root || d.main_leaf) ? 0 : (packed == 2 ? d.L_s : std::min(d.L_s, nt >= 1024 ? 256 : 128));
-    bytes = fp64 ? tile_smem_bytes<double>(La_rows, Lm_rows, oc, tv, false)
-                 : tile_smem_bytes<float>(La_rows, Lm_rows, oc, tv, packed == 1);
+    const int La_rows = d.aux_leaf ? d.nb * d.k : d.aux_cols;
+    const int Lm_rows = d.main_leaf ? 0 : d.main_cols;
+    // staged output columns: one coloring's L_s, or the launch's wide columns
+    // (nb row pitches) in chunks of a multiple of 4
+    const int wide = d.nb == 1 ? d.L_s : d.nb * d.s_cstride;
+    oc = (d.is_root || d.main_leaf) ? 0 : (packed == 2 ? d.L_s : std::min(wide, nt >= 1024 ? 256 : 128));
+    bytes = fp64 ? tile_smem_bytes<double>(La_rows, Lm_rows, oc, tv, false, d.nb)
+                 : tile_smem_bytes<float>(La_rows, Lm_rows, oc, tv, packed == 1, d.nb);
     if (bytes > limit) return false;
     if (!d.aux_leaf) {
         const int CH = fp64 ? 2 : 4;
-        const int nchunk = (d.L_a + CH - 1) / CH;
+        const int nchunk = (d.aux_cols + CH - 1) / CH;
         if (nchunk > 4 * nt) return false;
     }
     return true;

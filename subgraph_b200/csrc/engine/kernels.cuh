@@ -26,8 +26,9 @@ struct ColorArgs {
     const uint32_t *coef;      // [31][1024] coefficients of x^t mod P
     const uint32_t *window;    // [ncolorings][31] initial window per coloring
     const int32_t *perm;       // original -> internal vertex id
-    uint8_t *color;            // [ncolorings][V], internal order
+    uint8_t *color;            // internal order: coloring c, vertex v at c * color_stride + v * vertex_stride
     int64_t color_stride;
+    int64_t vertex_stride;     // 1: [ncolorings][V]; ncolorings: interleaved [V][ncolorings]
 };
 
 void launch_color(const ColorArgs &a, int ncolorings, cudaStream_t st);

@@ -10,14 +10,24 @@ enum CountMode : int32_t {
     kModeOriginal = 2,   // FP32 tables, isPruned=0 arithmetic (no scale, FP32 root)
 };
 
-// One sub-template step of one coloring: the fused aggregation + eMA over all
+// One sub-template step of nb colorings: the fused aggregation + eMA over all
 // vertices.  Tables are vertex-major: row v holds the v-th vertex's L columns
-// with a row pitch that is a multiple of 4 elements (16 B for FP32).
+// with a pitch that is a multiple of 4 elements (16 B for FP32).  A batch of
+// B colorings interleaves them per vertex: row v = [B][pitch] (row stride
+// B*pitch), colors [V][B]; a launch handles colorings [b0, b0 + nb) of it
+// (the table and color pointers are offset to b0).  The plain form is
+// B = nb = 1.
 struct StageDesc {
     int32_t V;
     int32_t L_s, S, L_m, L_a;          // L_m / L_a = k when that child is a leaf
-    int32_t out_pitch, main_pitch, aux_pitch;
+    int32_t out_pitch, main_pitch, aux_pitch;   // row strides (elements)
     int32_t k;
+    int32_t nb;                        // colorings of this launch
+    int32_t cstride;                   // color of (v, b) at color[v * cstride + b]
+    int32_t aux_cols, a_cstride;       // aux columns gathered per row; agg rows per coloring
+    int32_t main_cols, m_cstride;      // main columns loaded per row; main rows per coloring
+    int32_t out_w, s_cstride;          // columns written per row; output columns per coloring
+    int32_t rp_stride;                 // root partials per coloring
     int32_t main_leaf, aux_leaf;       // child of size 1: one-hot colors
     int32_t is_root;                   // sub 0: per-vertex root values, no table
     int32_t scaled;                    // first non-bottom sub: x 1e-12 through FP64
@@ -64,9 +74,10 @@ struct StageDesc {
 struct HubArgs {
     int32_t hub_count;
     int32_t chunk;
-    int32_t L_a, aux_pitch;      // aux row width / pitch (elements)
+    int32_t L_a, aux_pitch;      // aux columns summed per row / row stride (elements)
     int32_t row_pitch;           // pitch of the partial rows
-    int32_t k_leaf;              // > 0: the aux child is one-hot, count colors (k)
+    int32_t k_leaf;              // > 0: the aux child is one-hot, count colors (k) of nb colorings
+    int32_t nb, cstride;         // k_leaf: colorings, color layout (color[v * cstride + b])
     int32_t total_chunks;
     const uint8_t *color;        // [V] internal order (k_leaf only)
     const int32_t *chunk_start;  // [hub_count+1] first chunk index of each hub

@@ -89,13 +89,13 @@ constexpr int kPackedRow = 34;
 
 // Shared-memory layout of a tile: [La_rows][RS] aggregate, [Lm_rows][RS] main
 // rows (RS = TV+1, or kPackedRow for the packed eMA), [out_chunk][TV+1]
-// output staging, then TV doubles (root values) on a 16-byte boundary.
+// output staging, then nb*TV doubles (root values) on a 16-byte boundary.
 template <typename T>
-__host__ __device__ inline size_t tile_smem_bytes(int La_rows, int Lm_rows, int out_chunk, int tv, bool packed)
+__host__ __device__ inline size_t tile_smem_bytes(int La_rows, int Lm_rows, int out_chunk, int tv, bool packed, int nb = 1)
 {
     const size_t rs = packed ? (size_t)kPackedRow : (size_t)(tv + 1);
     size_t b = (((size_t)(La_rows + Lm_rows) * rs + (size_t)out_chunk * (size_t)(tv + 1)) * sizeof(T) + 15) & ~(size_t)15;
-    return b + (size_t)tv * sizeof(double);
+    return b + (size_t)nb * tv * sizeof(double);
 }
 
 // packed FP32x2 arithmetic (sm_100a): two independent lanes, each rounded
@@ -140,8 +140,9 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
     const int TV = d.tile_v;
     const int TVP = TV + 1;
     const int RS = PK ? kPackedRow : TVP;          // row stride of the aggregate and main rows
-    const int La_rows = d.aux_leaf ? d.k : d.L_a;
-    const int Lm_rows = d.main_leaf ? 0 : d.L_m;
+    const int nbc = d.nb;                          // colorings of this launch
+    const int La_rows = d.aux_leaf ? nbc * d.k : d.aux_cols;
+    const int Lm_rows = d.main_leaf ? 0 : d.main_cols;
     T *agg_s = reinterpret_cast<T *>(smem_raw);
     T *main_s = agg_s + (size_t)La_rows * RS;
     T *out_s = main_s + (size_t)Lm_rows * RS;
@@ -155,37 +156,81 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
 
     // ---- A: aggregation ------------------------------------------------------
     if (d.aux_leaf) {
-        // per-color neighbour counts, one thread per vertex (exact integers)
+        // per-color neighbour counts (row b*k + c for coloring b), one thread
+        // per vertex (exact integers)
+        const int nk = nbc * d.k;
+        const bool words = (nbc & 3) == 0 && (d.cstride & 3) == 0 &&   // 4 colorings per aligned load
+                           (reinterpret_cast<uintptr_t>(d.color) & 3) == 0;
         for (int vi = tid; vi < tv; vi += NT) {
-            for (int c = 0; c < d.k; ++c) agg_s[c * RS + vi] = T(0);
+            for (int c = 0; c < nk; ++c) agg_s[c * RS + vi] = T(0);
             const int v = v0 + vi;
             if (v < d.hub_count) {
                 const T *p = reinterpret_cast<const T *>(d.hub_partial);
                 const int c0 = __ldg(d.hub_chunk_start + v), c1 = __ldg(d.hub_chunk_start + v + 1);
                 for (int ch = c0; ch < c1; ++ch)
-                    for (int c = 0; c < d.k; ++c)
+                    for (int c = 0; c < nk; ++c)
                         agg_s[c * RS + vi] = add_rn(agg_s[c * RS + vi], ld_tab<COH>(p + (size_t)ch * d.hub_pitch + c));
                 continue;
             }
             const int beg = __ldg(d.off + v), end = __ldg(d.off + v + 1);
-            // batches of 8 neighbours, the last one predicated: every batch
-            // has its loads in flight together
-            for (int e = beg; e < end; e += 8) {
-                int nb[8], cl[8];
+            if (nbc == 1) {
+                // batches of 8 neighbours, the last one predicated: every batch
+                // has its loads in flight together
+                for (int e = beg; e < end; e += 8) {
+                    int nb[8], cl[8];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) nb[u] = e + u < end ? __ldg(d.adj + e + u) : -1;
+                    for (int u = 0; u < 8; ++u) nb[u] = e + u < end ? __ldg(d.adj + e + u) : -1;
 #pragma unroll
-                for (int u = 0; u < 8; ++u) cl[u] = nb[u] >= 0 ? (int)__ldg(d.color + nb[u]) : -1;
+                    for (int u = 0; u < 8; ++u) cl[u] = nb[u] >= 0 ? (int)__ldg(d.color + (size_t)nb[u] * d.cstride) : -1;
 #pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    if (cl[u] >= 0) agg_s[cl[u] * RS + vi] += T(1);
+                    for (int u = 0; u < 8; ++u)
+                        if (cl[u] >= 0) agg_s[cl[u] * RS + vi] += T(1);
+                }
+            } else if (words) {
+                // a neighbour's colors are nbc/4 32-bit words, taken 4 words
+                // (16 colorings) at a time for 4 neighbours at once
+                const int nw = nbc >> 2;
+                for (int e = beg; e < end; e += 4) {
+                    int nb[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) nb[u] = e + u < end ? __ldg(d.adj + e + u) : -1;
+                    for (int w0 = 0; w0 < nw; w0 += 4) {
+                        uint32_t cw[4][4];
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+#pragma unroll
+                            for (int w = 0; w < 4; ++w)
+                                cw[u][w] = (nb[u] >= 0 && w0 + w < nw)
+                                               ? __ldg(reinterpret_cast<const uint32_t *>(d.color + (size_t)nb[u] * d.cstride) +
+                                                       w0 + w)
+                                               : 0u;
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            if (nb[u] < 0) continue;
+#pragma unroll
+                            for (int w = 0; w < 4; ++w) {
+                                if (w0 + w >= nw) continue;
+#pragma unroll
+                                for (int i = 0; i < 4; ++i) {
+                                    const int c = (int)((cw[u][w] >> (8 * i)) & 0xffu);
+                                    agg_s[((4 * (w0 + w) + i) * d.k + c) * RS + vi] += T(1);
+                                }
+                            }
+                        }
+                    }
+                }
+            } else {
+                for (int e = beg; e < end; ++e) {
+                    const uint8_t *cp = d.color + (size_t)__ldg(d.adj + e) * d.cstride;
+                    for (int b = 0; b < nbc; ++b) agg_s[(b * d.k + __ldg(cp + b)) * RS + vi] += T(1);
+                }
             }
         }
     } else {
         const int G = d.gather_group;
         const int grp = tid / G, lane_g = tid - grp * G;
         const int ngrp = NT / G;
-        const int nchunk = (d.L_a + CH - 1) / CH;
+        const int nchunk = (d.aux_cols + CH - 1) / CH;
         const int rowc = d.aux_pitch / CH;
         const C *auxc = reinterpret_cast<const C *>(d.aux);
         if (grp < ngrp) {
@@ -236,7 +281,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
 #pragma unroll
                         for (int i = 0; i < CH; ++i) {
                             const int c = q * CH + i;
-                            if (c < d.L_a) agg_s[c * RS + vi] = CT::get(acc[r], i);
+                            if (c < d.aux_cols) agg_s[c * RS + vi] = CT::get(acc[r], i);
                         }
                     }
                 }
@@ -248,7 +293,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
         const T *mainp = reinterpret_cast<const T *>(d.main);
         for (int vi = warp; vi < tv; vi += NW) {
             const T *row = mainp + (size_t)(v0 + vi) * d.main_pitch;
-            for (int c = lane; c < d.L_m; c += 32) main_s[c * RS + vi] = ld_tab<COH>(row + c);
+            for (int c = lane; c < d.main_cols; c += 32) main_s[c * RS + vi] = ld_tab<COH>(row + c);
         }
     }
     __syncthreads();
@@ -259,70 +304,75 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
     const int VB = TV / VPW;                 // vertex blocks of the tile
     const int lv = lane % VPW, osub = lane / VPW;
     if (d.is_root) {
+        // root_s[b * TV + vi]: the root value of vertex vi in coloring b
         if (d.main_leaf) {
-            for (int vi = tid; vi < tv; vi += NT) {
-                const int cv = __ldg(d.color + v0 + vi);
+            for (int idx = tid; idx < nbc * tv; idx += NT) {
+                const int b = idx / tv, vi = idx - b * tv;
+                const int cv = __ldg(d.color + (size_t)(v0 + vi) * d.cstride + b);
                 const int r = __ldg(d.rem + cv);
-                root_s[vi] = r >= 0 ? (double)agg_s[r * RS + vi] : 0.0;
+                root_s[b * TV + vi] = r >= 0 ? (double)agg_s[(b * d.a_cstride + r) * RS + vi] : 0.0;
             }
         } else {
-            for (int b = warp; b < VB; b += NW) {
+            for (int u = warp; u < nbc * VB; u += NW) {
                 if (osub != 0) continue;
-                const int vi = b * VPW + lv;
+                const int cb = u / VB, vi = (u - cb * VB) * VPW + lv;
+                const T *mb = main_s + (size_t)cb * d.m_cstride * RS + vi;
+                const T *ab = agg_s + (size_t)cb * d.a_cstride * RS + vi;
                 double racc = 0.0;
                 float facc = 0.f;
                 for (int j = 0; j < d.S; ++j) {
                     const uint32_t pk = __ldg(d.split + (size_t)j * d.split_stride);
-                    const T x = main_s[(pk & 0xffffu) * RS + vi];
-                    const T y = agg_s[(pk >> 16) * RS + vi];
+                    const T x = mb[(pk & 0xffffu) * RS];
+                    const T y = ab[(pk >> 16) * RS];
                     if (sizeof(T) == 8) racc = __dadd_rn(racc, __dmul_rn((double)y, (double)x));
                     else if (d.root_float) facc = __fadd_rn(facc, __fmul_rn((float)y, (float)x));
                     else racc = __dadd_rn(racc, (double)__fmul_rn((float)y, (float)x));
                 }
-                if (vi < tv) root_s[vi] = (sizeof(T) == 4 && d.root_float) ? (double)facc : racc;
+                if (vi < tv) root_s[cb * TV + vi] = (sizeof(T) == 4 && d.root_float) ? (double)facc : racc;
             }
         }
         __syncthreads();
-        if (warp == 0) {
+        // one warp per coloring: the tile's vertices summed in a fixed order
+        for (int cb = warp; cb < nbc; cb += NW) {
             double s = 0.0;
             for (int vi = lane; vi < tv; vi += 32) {
-                s = __dadd_rn(s, root_s[vi]);
-                if (d.root_vertex) d.root_vertex[v0 + vi] = root_s[vi];
+                s = __dadd_rn(s, root_s[cb * TV + vi]);
+                if (d.root_vertex) d.root_vertex[v0 + vi] = root_s[cb * TV + vi];
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) s = __dadd_rn(s, __shfl_down_sync(0xffffffffu, s, o));
-            if (lane == 0) d.root_partial[tile] = s;
+            if (lane == 0) d.root_partial[(size_t)cb * d.rp_stride + tile] = s;
         }
     } else if (d.main_leaf) {
         // one-hot main: out[o] = agg[set(o) \ {color}] when color is in set(o)
+        // one flat, coalesced pass over the out_w written columns of the tile's
+        // rows (column t = coloring b, output o)
         T *outp = reinterpret_cast<T *>(d.out);
-        const int P = d.out_pitch;
-        // the tile's rows are contiguous: one flat, coalesced pass over them
-        const FastDiv fd = fast_div(P, tv * P);
-        T *tile_out = outp + (size_t)v0 * P;
-        for (int idx = tid; idx < tv * P; idx += NT) {
-            const int vi = fdiv(fd, idx), o = idx - vi * P;
+        const int P = d.out_pitch, W = d.out_w;
+        const FastDiv fd = fast_div(W, tv * W), fs = fast_div(d.s_cstride, W);
+        for (int idx = tid; idx < tv * W; idx += NT) {
+            const int vi = fdiv(fd, idx), t = idx - vi * W;
+            const int b = fdiv(fs, t), o = t - b * d.s_cstride;
             T val = T(0);
             if (o < d.L_s) {
-                const int cv = __ldg(d.color + v0 + vi);
+                const int cv = __ldg(d.color + (size_t)(v0 + vi) * d.cstride + b);
                 const int r = __ldg(d.rem + o * d.k + cv);
-                if (r >= 0) val = leaf_value(agg_s[r * RS + vi], scaled);
+                if (r >= 0) val = leaf_value(agg_s[(b * d.a_cstride + r) * RS + vi], scaled);
             }
-            tile_out[idx] = val;
+            outp[(size_t)(v0 + vi) * P + t] = val;
         }
     } else if (BLK && d.packed == 2) {
         // register-blocked eMA over all output columns at once (blk_ema.cuh),
         // then the rows of the tile written out contiguously
         if constexpr (BLK && sizeof(T) == 4 && !PK) {
             T *outp = reinterpret_cast<T *>(d.out);
-            const int P = d.out_pitch;
+            const int P = d.out_pitch, W = d.out_w;
             blk::ema_blocked(d, agg_s, main_s, out_s, RS, TVP, TV, warp, NW, lane);
             __syncthreads();
-            const FastDiv fd = fast_div(P, tv * P);
-            T *tile_out = outp + (size_t)v0 * P;
-            for (int idx = tid; idx < tv * P; idx += NT) {
-                const int vj = fdiv(fd, idx), t = idx - vj * P;
-                tile_out[idx] = t < d.L_s ? out_s[t * TVP + vj] : T(0);
+            const FastDiv fd = fast_div(W, tv * W);
+            for (int idx = tid; idx < tv * W; idx += NT) {
+                const int vj = fdiv(fd, idx), t = idx - vj * W;
+                outp[(size_t)(v0 + vj) * P + t] = t < d.L_s ? out_s[t * TVP + vj] : T(0);
             }
             __syncthreads();
         }
@@ -395,7 +445,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                 }
             }
             __syncthreads();
-            const int ow = (o0 + oc == d.L_s) ? P - o0 : oc;
+            const int ow = (o0 + oc == d.L_s) ? d.out_w - o0 : oc;
             const FastDiv fd = fast_div(ow, tv * ow);
             for (int idx = tid; idx < tv * ow; idx += NT) {
                 const int vj = fdiv(fd, idx), t = idx - vj * ow;
@@ -406,19 +456,32 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
     } else {
         // each lane accumulates 4 consecutive output columns of its vertex at once
         // (4 independent chains); the split table is stored [j][column] so one
-        // 16-byte warp-uniform load gives the 4 (main, aux) pairs of split j
+        // 16-byte warp-uniform load gives the 4 (main, aux) pairs of split j.
+        // Columns are "wide": w = b * s_cstride + o over the launch's colorings
+        // (one coloring: w = o < L_s, the row padding filled at the end).
         T *outp = reinterpret_cast<T *>(d.out);
         const int P = d.out_pitch;
         const int SP = d.split_stride;
-        for (int o0 = 0; o0 < d.L_s; o0 += d.out_chunk) {
-            const int oc = min(d.out_chunk, d.L_s - o0);
+        const int WW = nbc == 1 ? d.L_s : nbc * d.s_cstride;
+        const FastDiv fs = fast_div(d.s_cstride, WW);
+        for (int o0 = 0; o0 < WW; o0 += d.out_chunk) {
+            const int oc = min(d.out_chunk, WW - o0);
             const int ngroups = (oc + 4 * OPI - 1) / (4 * OPI);
             for (int unit = warp; unit < VB * ngroups; unit += NW) {
-                const int b = unit % VB, og = unit / VB;
+                const int vb = unit % VB, og = unit / VB;
                 const int ol = (og * OPI + osub) * 4;
                 if (ol >= oc) continue;
-                const int vi = b * VPW + lv;
-                const uint4 *sp = reinterpret_cast<const uint4 *>(d.split + o0 + ol);
+                const int vi = vb * VPW + lv;
+                const int w = o0 + ol;
+                const int b = nbc == 1 ? 0 : fdiv(fs, w), o = w - b * d.s_cstride;
+                if (o >= d.L_s) {   // a group of row padding (several colorings)
+                    for (int u = 0; u < 4; ++u)
+                        if (ol + u < oc) out_s[(ol + u) * TVP + vi] = T(0);
+                    continue;
+                }
+                const T *mb = main_s + (size_t)b * d.m_cstride * RS + vi;
+                const T *ab = agg_s + (size_t)b * d.a_cstride * RS + vi;
+                const uint4 *sp = reinterpret_cast<const uint4 *>(d.split + o);
                 const size_t sstep = (size_t)(SP / 4);
                 T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
                 int j = 0;
@@ -431,10 +494,10 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                     T ag[4][4], mn[4][4];
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
-                        ag[u][0] = agg_s[(pk[u].x >> 16) * RS + vi]; mn[u][0] = main_s[(pk[u].x & 0xffffu) * RS + vi];
-                        ag[u][1] = agg_s[(pk[u].y >> 16) * RS + vi]; mn[u][1] = main_s[(pk[u].y & 0xffffu) * RS + vi];
-                        ag[u][2] = agg_s[(pk[u].z >> 16) * RS + vi]; mn[u][2] = main_s[(pk[u].z & 0xffffu) * RS + vi];
-                        ag[u][3] = agg_s[(pk[u].w >> 16) * RS + vi]; mn[u][3] = main_s[(pk[u].w & 0xffffu) * RS + vi];
+                        ag[u][0] = ab[(pk[u].x >> 16) * RS]; mn[u][0] = mb[(pk[u].x & 0xffffu) * RS];
+                        ag[u][1] = ab[(pk[u].y >> 16) * RS]; mn[u][1] = mb[(pk[u].y & 0xffffu) * RS];
+                        ag[u][2] = ab[(pk[u].z >> 16) * RS]; mn[u][2] = mb[(pk[u].z & 0xffffu) * RS];
+                        ag[u][3] = ab[(pk[u].w >> 16) * RS]; mn[u][3] = mb[(pk[u].w & 0xffffu) * RS];
                     }
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
@@ -446,18 +509,20 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                 }
                 for (; j < d.S; ++j) {
                     const uint4 pk = __ldg(sp + (size_t)j * sstep);
-                    a0 = ema_step(a0, agg_s[(pk.x >> 16) * RS + vi], main_s[(pk.x & 0xffffu) * RS + vi], scaled);
-                    a1 = ema_step(a1, agg_s[(pk.y >> 16) * RS + vi], main_s[(pk.y & 0xffffu) * RS + vi], scaled);
-                    a2 = ema_step(a2, agg_s[(pk.z >> 16) * RS + vi], main_s[(pk.z & 0xffffu) * RS + vi], scaled);
-                    a3 = ema_step(a3, agg_s[(pk.w >> 16) * RS + vi], main_s[(pk.w & 0xffffu) * RS + vi], scaled);
+                    a0 = ema_step(a0, ab[(pk.x >> 16) * RS], mb[(pk.x & 0xffffu) * RS], scaled);
+                    a1 = ema_step(a1, ab[(pk.y >> 16) * RS], mb[(pk.y & 0xffffu) * RS], scaled);
+                    a2 = ema_step(a2, ab[(pk.z >> 16) * RS], mb[(pk.z & 0xffffu) * RS], scaled);
+                    a3 = ema_step(a3, ab[(pk.w >> 16) * RS], mb[(pk.w & 0xffffu) * RS], scaled);
                 }
-                out_s[ol * TVP + vi] = a0;
-                if (ol + 1 < oc) out_s[(ol + 1) * TVP + vi] = a1;
-                if (ol + 2 < oc) out_s[(ol + 2) * TVP + vi] = a2;
-                if (ol + 3 < oc) out_s[(ol + 3) * TVP + vi] = a3;
+                // columns past L_s inside the group are row padding: zero
+                const T av[4] = {a0, a1, a2, a3};
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (ol + u < oc) out_s[(ol + u) * TVP + vi] = o + u < d.L_s ? av[u] : T(0);
             }
             __syncthreads();
-            const int ow = (o0 + oc == d.L_s) ? P - o0 : oc;   // the last chunk zero-fills the row padding
+            // one coloring: the last chunk zero-fills the row padding up to out_w
+            const int ow = (nbc == 1 && o0 + oc == d.L_s) ? d.out_w - o0 : oc;
             const FastDiv fd = fast_div(ow, tv * ow);
             for (int idx = tid; idx < tv * ow; idx += NT) {
                 const int vj = fdiv(fd, idx), t = idx - vj * ow;
@@ -493,12 +558,17 @@ __device__ __forceinline__ void hub_item(const HubArgs &h, int item, unsigned ch
     const int end = min(__ldg(h.off + v + 1), beg + h.chunk);
     T *prow = reinterpret_cast<T *>(h.partial) + (size_t)item * h.row_pitch;
     if (h.k_leaf) {
+        // colour counts of the chunk's neighbours, k per coloring (nb * k <= 256)
+        const int nk = h.nb * h.k_leaf;
         uint32_t *cnt = reinterpret_cast<uint32_t *>(smem_raw);
-        if (threadIdx.x < 32) cnt[threadIdx.x] = 0;
+        for (int i = threadIdx.x; i < nk; i += NT) cnt[i] = 0;
         __syncthreads();
-        for (int e = beg + (int)threadIdx.x; e < end; e += NT) atomicAdd(&cnt[__ldg(h.color + __ldg(h.adj + e))], 1u);
+        for (int e = beg + (int)threadIdx.x; e < end; e += NT) {
+            const uint8_t *cp = h.color + (size_t)__ldg(h.adj + e) * h.cstride;
+            for (int b = 0; b < h.nb; ++b) atomicAdd(&cnt[b * h.k_leaf + __ldg(cp + b)], 1u);
+        }
         __syncthreads();
-        if ((int)threadIdx.x < h.k_leaf) prow[threadIdx.x] = (T)cnt[threadIdx.x];
+        for (int i = threadIdx.x; i < nk; i += NT) prow[i] = (T)cnt[i];
         __syncthreads();
         return;
     }
