@@ -179,7 +179,9 @@ def run_reference_arm(args, w):
 def config_of(args, w):
     return {"workload": args.workload, "graph": f"rmat scale {w['scale']} edge factor {w['ef']} seed 1",
             "template": w["template"], "colorings_per_step": w["per_step"], "tables": "fp32",
-            "sums": "fp64", "form": "plain" if args.batch == 0 else f"batched({args.batch})",
+            "sums": "fp64",
+            "form": "plain" if args.batch == 0 else (f"persistent({args.batch})" if args.persistent
+                                                     else f"interleaved groups({args.batch})"),
             "hub_threshold": args.hub, "l2": "inputs larger than L2 (count tables of several GB per coloring)"}
 
 
@@ -190,7 +192,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
-    ap.add_argument("--batch", type=int, default=0, help="colorings per persistent launch (0 = plain)")
+    ap.add_argument("--batch", type=int, default=0, help="colorings per batch (0 = plain form)")
+    ap.add_argument("--persistent", action="store_true", help="batched form: persistent work-queue launch per batch")
     ap.add_argument("--hub", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -241,7 +244,7 @@ def main():
         return w["seed"] + (step * world + rank) * B
 
     for s in range(args.warmup):
-        sg.count(g, tmpl, B, seeds(s), batch=args.batch, hub_threshold=args.hub)
+        sg.count(g, tmpl, B, seeds(s), batch=args.batch, hub_threshold=args.hub, persistent=args.persistent)
     barrier()
     dev_ms, launches, fused_ms, fused_launches, fused_bytes, gather_bytes, hub_ms = 0.0, 0, 0.0, 0, 0.0, 0.0, 0.0
     raws = []
@@ -250,7 +253,7 @@ def main():
         torch.cuda.nvtx.range_push("timed")
         for s in range(args.steps):
             raw, st = sg.count(g, tmpl, B, seeds(args.warmup + s), batch=args.batch, hub_threshold=args.hub,
-                               return_stats=True, profile=True)
+                               persistent=args.persistent, return_stats=True, profile=True)
             raws.append(raw)
             dev_ms += st["device_ms"]
             launches += st["kernel_launches"]
@@ -295,7 +298,8 @@ def main():
         t0 = time.perf_counter()
         for s in range(args.steps):
             dg = sg.DeviceGraph(col_np, row_np, local)
-            sg.count(dg, tmpl, B, seeds(args.warmup + s), batch=args.batch, hub_threshold=args.hub)
+            sg.count(dg, tmpl, B, seeds(args.warmup + s), batch=args.batch, hub_threshold=args.hub,
+                     persistent=args.persistent)
             del dg
         barrier()
         e2e_s = max_over_ranks(time.perf_counter() - t0)
