@@ -53,7 +53,43 @@ WORKLOADS = {
     # enough for full ncu captures (about 2 GB of tables, still above L2)
     "tree12_rmat18_ef8": dict(scale=18, ef=8, template="tree12", per_step=1, seed=7),
 }
+# a seeded stream of 256 jobs, each a random tree of 3-10 vertices (uniform
+# Pruefer sequence, smallest-leaf decoding, edges in decode order) on one of
+# three R-MAT graphs (scales 16, 18, 20, edge factor 8): one coloring per job,
+# the jobs of a graph in persistent job-queue launches
+MIXED = dict(jobs=256, stream_seed=5, scales=(16, 18, 20), ef=8, seed=7)
+WORKLOADS["mixed256_rmat16_18_20_ef8"] = dict(mixed=True, per_step=MIXED["jobs"], template="random 3-10",
+                                              scale="16/18/20", ef=8, seed=7)
 DEFAULT_WORKLOAD = "tree12_rmat20_ef8"
+
+
+def prufer_tree(n, rng):
+    """Edges of the labelled tree of a uniform random Pruefer sequence."""
+    if n == 2:
+        return [(0, 1)]
+    seq = [rng.randrange(n) for _ in range(n - 2)]
+    deg = [1] * n
+    for a in seq:
+        deg[a] += 1
+    edges = []
+    for a in seq:
+        leaf = min(i for i in range(n) if deg[i] == 1)
+        edges.append((leaf, a))
+        deg[leaf] -= 1
+        deg[a] -= 1
+    u, v = [i for i in range(n) if deg[i] == 1]
+    edges.append((u, v))
+    return edges
+
+
+def mixed_jobs():
+    import random
+    rng = random.Random(MIXED["stream_seed"])
+    jobs = []
+    for j in range(MIXED["jobs"]):
+        n = rng.randint(3, 10)
+        jobs.append((rng.randrange(len(MIXED["scales"])), n, prufer_tree(n, rng), MIXED["seed"] + j))
+    return jobs
 METRIC = "colorings/sec"
 
 
@@ -176,6 +212,109 @@ def run_reference_arm(args, w):
     print(json.dumps(line), flush=True)
 
 
+def run_mixed(args):
+    """The mixed-template job stream: every step counts all jobs once."""
+    import numpy as np
+    import torch
+
+    import subgraph_b200 as sg
+    jobs = mixed_jobs()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    cfg = {"workload": args.workload, "jobs": MIXED["jobs"], "templates": "random trees of 3-10 vertices",
+           "graphs": "rmat scales 16/18/20 edge factor 8 seed 1", "stream_seed": MIXED["stream_seed"],
+           "form": "persistent job queue per graph", "tables": "fp32", "sums": "fp64",
+           "l2": "inputs larger than L2 at scales 18 and 20"}
+    graphs = []
+    for sc in MIXED["scales"]:
+        el = sg.rmat(sc, MIXED["ef"], seed=1)
+        csc = sg.CSCGraph()
+        csc.createFromEdgeListFile(el.getNumVertices(), el.getNumEdges(), el.getSrcList(), el.getDstList())
+        graphs.append(csc)
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        # the reference CLI on a bounded sample: the first jobs of the stream, one coloring each
+        t_tot, done = 0.0, 0
+        with tempfile.TemporaryDirectory() as tmp:
+            for gi, n, edges, seed in jobs:
+                if t_tot > 20.0 or done >= 32:
+                    break
+                w = dict(template=f"job{done}", seed=seed)
+                TEMPLATES[w["template"]] = (n, edges)
+                sec, kind, cores = reference_cpu(w, graphs[gi], 1, os.cpu_count() or 1, tmp)
+                t_tot += sec
+                done += 1
+        value = done / t_tot
+        print(json.dumps({"metric": METRIC, "value": value, "unit": "colorings/s", "impl": "reference",
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": MIXED["jobs"] / value * 1000.0, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "fp32", "data": "synthetic", "config": cfg,
+                          "cpu_baseline": {"value": value, "unit": "colorings/s", "cores": cores, "kind": kind,
+                                           "sample": f"the first {done} jobs of the stream, one coloring each"},
+                          "e2e": {"value": value, "unit": "colorings/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dgs = [csc.device_graph(local) for csc in graphs]
+    tmpls = [sg.Graph(n, e) for _, n, e, _ in jobs]
+    by_graph = [[j for j, job in enumerate(jobs) if job[0] == gi] for gi in range(len(graphs))]
+
+    def step():
+        ms, lat = 0.0, np.zeros(len(jobs))
+        raw = np.zeros(len(jobs))
+        for gi, idx in enumerate(by_graph):
+            if not idx:
+                continue
+            r, l, st = sg.count_jobs(dgs[gi], [tmpls[j] for j in idx], [jobs[j][3] for j in idx],
+                                     return_latency=True, return_stats=True)
+            raw[idx], lat[idx] = r, l + ms   # the graphs run one after the other
+            ms += st["device_ms"]
+        return ms, lat, raw
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    tot, lats = 0.0, []
+    with Clocks(local) as clk:
+        torch.cuda.nvtx.range_push("timed")
+        for _ in range(args.steps):
+            ms, lat, raw = step()
+            tot += ms
+            lats.append(lat)
+        torch.cuda.nvtx.range_pop()
+    clocks = clk.summary()
+    value = world * len(jobs) * args.steps / (tot / 1000.0)
+    lat = np.concatenate(lats)
+    # the plain form: each job on its own, one after the other
+    plain_ms = 0.0
+    for j, (gi, n, e, seed) in enumerate(jobs):
+        _, st = sg.count(dgs[gi], tmpls[j], 1, seed, return_stats=True)
+    for j, (gi, n, e, seed) in enumerate(jobs):
+        _, st = sg.count(dgs[gi], tmpls[j], 1, seed, return_stats=True)
+        plain_ms += st["device_ms"]
+    plain = len(jobs) / (plain_ms / 1000.0)
+    # end to end: graphs already resident, templates planned on the host each step
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for gi, idx in enumerate(by_graph):
+            ts = [sg.Graph(jobs[j][1], jobs[j][2]) for j in idx]
+            sg.count_jobs(dgs[gi], ts, [jobs[j][3] for j in idx])
+    e2e_s = time.perf_counter() - t0
+    line = {"metric": METRIC, "value": value, "unit": "colorings/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tot / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32", "data": "synthetic", "config": cfg,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "forms": {"plain": plain, "batched": value, "batched_over_plain": value / plain, "unit": "colorings/s"},
+            "roofline": None, "gpu_launches": None, "clocks": clocks,
+            "e2e": {"value": world * len(jobs) * args.steps / e2e_s, "unit": "colorings/s",
+                    "h2d_bytes_per_step": 124 * len(jobs),   # one 31-word coloring window per job
+                    "d2h_bytes_per_step": 16 * len(jobs)}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def config_of(args, w):
     return {"workload": args.workload, "graph": f"rmat scale {w['scale']} edge factor {w['ef']} seed 1",
             "template": w["template"], "colorings_per_step": w["per_step"], "tables": "fp32",
@@ -200,6 +339,9 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip timing the other form (plain vs batched)")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
+    if w.get("mixed"):
+        run_mixed(args)
+        return
     if args.impl == "reference":
         run_reference_arm(args, w)
         return

@@ -152,6 +152,17 @@ void sg_count_opts_default(sg_count_opts *o);
  * counts, one per coloring, into raw[n_colorings] (host). */
 sg_status sg_count(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw, sg_count_stats *stats);
 
+/* A stream of jobs with different templates on one graph: job j counts one
+ * coloring of plans[j] seeded srand(seeds[j]) into raw[j].  The jobs run as
+ * persistent work-queue launches (all their sub-template stages in one queue,
+ * waves admitted by free device memory).  From opts: mode, hub_threshold,
+ * exact, wait_limit_ms.  job_ms (optional, n_jobs): each job's latency from
+ * the start of its wave's launch to the end of its last stage.  The reference
+ * runs one template per CountMat::compute (CountMat.cpp:79-266); this is the
+ * batched mixed-template form with no single counterpart there. */
+sg_status sg_count_jobs(sg_graph g, int32_t n_jobs, const sg_plan *plans, const uint32_t *seeds,
+                        const sg_count_opts *opts, double *raw, double *job_ms, sg_count_stats *stats);
+
 /* CountMat::compute's final estimate (CountMat.cpp:246-264):
  * floor(mean(raw) / (k!/k^k * automorphisms) + 0.5). */
 sg_status sg_estimate(const double *raw, int32_t n, int32_t k, int32_t automorphisms, double *out);

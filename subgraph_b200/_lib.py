@@ -31,7 +31,7 @@ EXPORTS = [
     "sg_plan_create", "sg_plan_read", "sg_plan_destroy", "sg_plan_info", "sg_plan_sub",
     "sg_plan_tables", "sg_plan_automorphisms", "sg_plan_sub_edges",
     "sg_graph_create", "sg_graph_destroy", "sg_graph_info",
-    "sg_count_opts_default", "sg_count", "sg_estimate",
+    "sg_count_opts_default", "sg_count", "sg_count_jobs", "sg_estimate",
     "sg_colors", "sg_debug_sub_table", "sg_debug_root", "sg_colors_noalloc",
     "sg_countmat_create", "sg_countmat_destroy", "sg_countmat_initialization",
     "sg_countmat_set_seed", "sg_countmat_compute", "sg_countmat_raw",
@@ -97,6 +97,7 @@ def lib() -> ctypes.CDLL:
         "sg_graph_info": ([vp, P(i32), P(i64), P(i32)], i32),
         "sg_count_opts_default": ([P(CountOpts)], None),
         "sg_count": ([vp, vp, P(CountOpts), vp, P(CountStats)], i32),
+        "sg_count_jobs": ([vp, i32, vp, vp, P(CountOpts), vp, vp, P(CountStats)], i32),
         "sg_estimate": ([vp, i32, i32, i32, P(d)], i32),
         "sg_colors": ([vp, i32, u32, vp], i32),
         "sg_debug_sub_table": ([vp, vp, u32, i32, i32, i32, vp], i32),

@@ -423,6 +423,35 @@ def count(graph: DeviceGraph, template: Graph, n_colorings: int = 1, seed_base: 
     return raw
 
 
+def count_jobs(graph: DeviceGraph, templates, seeds, mode: int = MODE_REFERENCE, hub_threshold: int = 1024,
+               exact: bool = False, wait_limit_ms: int = 0, return_latency: bool = False, return_stats: bool = False):
+    """One coloring each of jobs with different templates on one graph (job j:
+    templates[j] seeded srand(seeds[j])), in persistent work-queue launches.
+    Returns the raw counts; with return_latency also each job's latency (ms)."""
+    n = len(templates)
+    if n != len(seeds):
+        raise ValueError("one seed per job")
+    plans = (ctypes.c_void_p * n)(*[t.plan for t in templates])
+    sd = np.ascontiguousarray([int(x) & 0xFFFFFFFF for x in seeds], np.uint32)
+    o = CountOpts()
+    lib().sg_count_opts_default(ctypes.byref(o))
+    o.mode = mode
+    o.hub_threshold = hub_threshold
+    o.exact = 1 if exact else 0
+    o.wait_limit_ms = wait_limit_ms
+    raw = np.zeros(n, np.float64)
+    lat = np.zeros(n, np.float64)
+    st = CountStats()
+    check(lib().sg_count_jobs(graph.handle, n, ctypes.cast(plans, ctypes.c_void_p), _p(sd), ctypes.byref(o), _p(raw),
+                              _p(lat), ctypes.byref(st)))
+    out = [raw]
+    if return_latency:
+        out.append(lat)
+    if return_stats:
+        out.append({k: getattr(st, k) for k, _ in CountStats._fields_})
+    return out[0] if len(out) == 1 else tuple(out)
+
+
 def estimate(raw: Sequence[float], k: int, automorphisms: int = 1) -> float:
     r = np.ascontiguousarray(raw, np.float64)
     out = ctypes.c_double()
@@ -494,5 +523,5 @@ class CountMat:
 
 
 __all__ = ["EdgeList", "CSCGraph", "CSRGraph", "DeviceGraph", "Graph", "DivideTemplates", "IndexSys", "CountMat",
-           "count", "estimate", "rmat", "debug_sub_table", "debug_root", "MODE_REFERENCE", "MODE_FP64",
+           "count", "count_jobs", "estimate", "rmat", "debug_sub_table", "debug_root", "MODE_REFERENCE", "MODE_FP64",
            "MODE_ORIGINAL", "DUMMY_VAL", "SGError"]

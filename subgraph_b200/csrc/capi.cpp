@@ -336,6 +336,35 @@ sg_status sg_count(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw, s
     SG_GUARD_END
 }
 
+sg_status sg_count_jobs(sg_graph g, int32_t n_jobs, const sg_plan *plans, const uint32_t *seeds,
+                        const sg_count_opts *o, double *raw, double *job_ms, sg_count_stats *stats)
+{
+    SG_GUARD_BEGIN
+    if (!g || !plans || !seeds || !o || !raw) return fail(SG_ERR_INVALID, "null argument");
+    if (n_jobs < 1) return fail(SG_ERR_INVALID, "n_jobs must be >= 1");
+    std::vector<const sg::Plan *> ps((size_t)n_jobs);
+    for (int32_t j = 0; j < n_jobs; ++j) {
+        if (!plans[j]) return fail(SG_ERR_INVALID, "null plan in the job list");
+        ps[j] = &plans[j]->p;
+    }
+    sg::CountOptions co;
+    co.mode = o->mode;
+    co.hub_threshold = o->hub_threshold;
+    co.exact = o->exact ? 1 : 0;
+    co.wait_limit_ms = o->wait_limit_ms;
+    sg::CountStats cs;
+    sg_status st = from(sg::count_jobs(*g->g, ps, seeds, co, raw, job_ms, &cs));
+    if (st) return st;
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->device_ms = cs.device_ms;
+        stats->kernel_launches = cs.kernel_launches;
+        stats->table_bytes = cs.table_bytes;
+    }
+    return SG_OK;
+    SG_GUARD_END
+}
+
 static int factorial_int(int n) { return n <= 1 ? 1 : n * factorial_int(n - 1); }
 
 sg_status sg_estimate(const double *raw, int32_t n, int32_t k, int32_t automorphisms, double *out)

@@ -15,6 +15,13 @@
 
 namespace sg {
 
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 __device__ __forceinline__ int ld_acquire(const int *p)
 {
     int v;
@@ -44,13 +51,16 @@ __device__ __forceinline__ void batch_fused(const StageDesc &d, int tile, unsign
 template <typename T>
 __global__ void __launch_bounds__(kBatchThreads, 1)
     k_persistent(const BatchStage *__restrict__ stages, int nstages, int total_items, int *done, BatchCtl *ctl,
-                 long long wait_cycles)
+                 long long wait_cycles, unsigned long long *stage_end)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ BatchStage st;
     __shared__ int s_item, s_stage, s_skip;
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(&ctl->next_item, 1);
+        if (threadIdx.x == 0) {
+            s_item = atomicAdd(&ctl->next_item, 1);
+            if (s_item == 0 && stage_end) ctl->t0 = global_ns();
+        }
         __syncthreads();
         const int item = s_item;
         if (item >= total_items) break;
@@ -97,18 +107,21 @@ __global__ void __launch_bounds__(kBatchThreads, 1)
         __syncthreads();
         if (threadIdx.x == 0) {
             __threadfence();
-            atomicAdd(done + s_stage, 1);
+            const int prev = atomicAdd(done + s_stage, 1);
+            // the CTA that completes a stage stamps its end (job latencies)
+            if (stage_end && prev + 1 == st.nitems) stage_end[s_stage] = global_ns();
         }
     }
 }
 
 // per-slot root sums of a batch (one CTA per coloring slot), FP64 Kahan in a
 // fixed order like k_root_reduce
-__global__ void k_root_reduce_slots(const double *__restrict__ partial, int64_t slot_stride, int32_t n, double scale,
-                                    double *out)
+__global__ void k_root_reduce_slots(const double *__restrict__ partial, int64_t slot_stride, int32_t n,
+                                    const int32_t *__restrict__ n_slot, double scale, double *out)
 {
     __shared__ double ss[256], cc[256];
     const double *p = partial + (size_t)blockIdx.x * slot_stride;
+    if (n_slot) n = n_slot[blockIdx.x];   // jobs of different templates: their own tile counts
     double s = 0.0, c = 0.0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const double y = __dadd_rn(p[i], -c);
@@ -130,11 +143,12 @@ __global__ void k_root_reduce_slots(const double *__restrict__ partial, int64_t 
 }
 
 cudaError_t launch_persistent(const BatchStage *stages, int nstages, int total_items, int *done, BatchCtl *ctl,
-                              long long wait_cycles, size_t smem, bool fp64, int sm_count, cudaStream_t st)
+                              long long wait_cycles, size_t smem, bool fp64, int sm_count, cudaStream_t st,
+                              unsigned long long *stage_end)
 {
     auto go = [&](auto kern) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kern<<<sm_count, kBatchThreads, smem, st>>>(stages, nstages, total_items, done, ctl, wait_cycles);
+        kern<<<sm_count, kBatchThreads, smem, st>>>(stages, nstages, total_items, done, ctl, wait_cycles, stage_end);
     };
     if (fp64) go(k_persistent<double>);
     else go(k_persistent<float>);
@@ -142,9 +156,9 @@ cudaError_t launch_persistent(const BatchStage *stages, int nstages, int total_i
 }
 
 void launch_root_reduce_slots(const double *partial, int64_t slot_stride, int32_t n, double scale, double *out,
-                              int nslots, cudaStream_t st)
+                              int nslots, cudaStream_t st, const int32_t *n_slot)
 {
-    if (nslots > 0) k_root_reduce_slots<<<nslots, 256, 0, st>>>(partial, slot_stride, n, scale, out);
+    if (nslots > 0) k_root_reduce_slots<<<nslots, 256, 0, st>>>(partial, slot_stride, n, n_slot, scale, out);
 }
 
 }  // namespace sg

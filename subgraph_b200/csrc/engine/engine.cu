@@ -527,6 +527,7 @@ struct RunCtx {
     bool autotune = false;
     bool blocked = true;     // register-blocked eMA allowed
     int lay = 1;             // colorings interleaved per table row (grouped batched form)
+    size_t arena_base = 0;   // byte offset of this context's tables in the arena (job queues)
     bool exact = false;      // no fused products (packed eMA), no hub chunks
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> fused_ev, hub_ev;
     double fused_alg_bytes = 0, fused_gather_bytes = 0;
@@ -589,7 +590,7 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
 // the table is [V][lay][pitch] at lay times the per-coloring offset.
 void *table_ptr(RunCtx &c, int slot, int sub)
 {
-    return (char *)c.gs.ws.arena + c.arena_per_coloring * slot +
+    return (char *)c.gs.ws.arena + c.arena_base + c.arena_per_coloring * slot +
            (size_t)c.lay * c.p.table_offset[sub] * c.g.V * c.es;
 }
 
@@ -823,6 +824,74 @@ bool batch_shape(StageDesc &d, bool fp64)
     return false;
 }
 
+// The queue stages of one coloring slot of context c: per sub (in processing
+// order, one call per sub) the hub chunks (when the graph has hubs) and the
+// fused tile groups.  `fused` / `hub` map the slot's subs to stage indices;
+// `hub_region` is this (slot, sub)'s partial-row buffer.
+struct QueueSlot {
+    std::vector<int> proc_index, fused, hub;
+    int root_tiles = 0;
+    explicit QueueSlot(const Plan &p) : proc_index(p.nsub(), -1), fused(p.nsub(), -1), hub(p.nsub(), -1)
+    {
+        for (size_t i = 0; i < p.process_order.size(); ++i) proc_index[p.process_order[i]] = (int)i;
+    }
+};
+
+Status add_queue_stage(RunCtx &c, int slot, int s, void *hub_region, QueueSlot &q, std::vector<BatchStage> &S,
+                       int &item, size_t &smem)
+{
+    const Plan &p = c.p;
+    const SubTemplate &sub = p.subs[s];
+    StageDesc d = make_stage(c, slot, s, nullptr);
+    if (c.hubs.count > 0) {
+        BatchStage hs{};
+        hs.kind = kStageHub;
+        hs.h = make_hub(c, d, hub_region);
+        hs.first_item = item;
+        hs.nitems = c.hubs.total_chunks;
+        if (p.subs[sub.aux].size > 1) hs.deps[hs.ndeps++] = q.fused[sub.aux];
+        item += hs.nitems;
+        q.hub[s] = (int)S.size();
+        S.push_back(hs);
+    }
+    if (!batch_shape(d, c.fp64))
+        return Status{6, "sub-template " + std::to_string(s) + " needs more shared memory than a CTA has"};
+    BatchStage fs{};
+    fs.kind = kStageFused;
+    fs.d = d;
+    fs.tiles_per_item = std::max(1, 1024 / d.tile_v);
+    fs.first_item = item;
+    fs.nitems = (d.ntiles + fs.tiles_per_item - 1) / fs.tiles_per_item;
+    std::vector<int> deps;
+    if (p.subs[sub.main].size > 1) deps.push_back(q.fused[sub.main]);
+    if (p.subs[sub.aux].size > 1) deps.push_back(q.fused[sub.aux]);
+    if (c.hubs.count > 0) deps.push_back(q.hub[s]);
+    // write after read: the arena gives this table the range of tables
+    // already consumed; their consumers may still be reading it
+    if (s != 0) {
+        const int64_t lo = p.table_offset[s], hi = lo + p.table_pitch[s];
+        for (int x : p.process_order) {
+            if (x == s) break;
+            const int par = p.subs[x].parent;
+            if (x == 0 || par < 0 || par >= p.nsub() || q.proc_index[par] >= q.proc_index[s]) continue;
+            const int64_t xlo = p.table_offset[x], xhi = xlo + p.table_pitch[x];
+            if (xlo < hi && lo < xhi) {
+                const int dep = q.fused[par];
+                if (std::find(deps.begin(), deps.end(), dep) == deps.end()) deps.push_back(dep);
+            }
+        }
+    }
+    if ((int)deps.size() > kBatchMaxDeps)
+        return Status{6, "sub-template " + std::to_string(s) + " needs more queue dependencies than a stage holds"};
+    for (int dep : deps) fs.deps[fs.ndeps++] = dep;
+    item += fs.nitems;
+    smem = std::max(smem, d.smem);
+    if (s == 0) q.root_tiles = d.ntiles;
+    q.fused[s] = (int)S.size();
+    S.push_back(fs);
+    return Status::ok();
+}
+
 // Builds the work queue of a batch of `slots` colorings: for every sub in
 // processing order and every slot, the hub chunks (when the graph has hubs)
 // and the fused tile groups of that (slot, sub) stage.
@@ -831,71 +900,24 @@ Status build_batch(RunCtx &c, int slots, bool poison, BatchPlan &bp)
     const Plan &p = c.p;
     DeviceGraph &g = c.g;
     const int nproc = (int)p.process_order.size();
-    std::vector<int> proc_index(p.nsub(), -1);
-    for (int i = 0; i < nproc; ++i) proc_index[p.process_order[i]] = i;
     const size_t hub_region = (size_t)c.hubs.total_chunks * (size_t)std::max(c.hub_pitch, 4) * c.es;
     if (c.hubs.count > 0) {
         const size_t bytes = std::max<size_t>(16, hub_region * (size_t)slots * nproc);
         SG_CK(cudaMallocAsync(&bp.d_hub, bytes, g.stream));
     }
-    std::vector<int> fused_stage((size_t)slots * p.nsub(), -1), hub_stage((size_t)slots * p.nsub(), -1);
+    std::vector<QueueSlot> qs(slots, QueueSlot(p));
     std::vector<BatchStage> &S = bp.host_stages;
     S.clear();
     int item = 0;
     size_t smem = (size_t)kBatchThreads * 16;   // hub items' lane partials
-    for (int s : p.process_order) {
-        const SubTemplate &sub = p.subs[s];
+    for (int s : p.process_order)
         for (int b = 0; b < slots; ++b) {
-            StageDesc d = make_stage(c, b, s, nullptr);
-            if (c.hubs.count > 0) {
-                void *region = (char *)bp.d_hub + hub_region * ((size_t)b * nproc + proc_index[s]);
-                BatchStage hs{};
-                hs.kind = kStageHub;
-                hs.h = make_hub(c, d, region);
-                hs.first_item = item;
-                hs.nitems = c.hubs.total_chunks;
-                if (p.subs[sub.aux].size > 1) hs.deps[hs.ndeps++] = fused_stage[(size_t)b * p.nsub() + sub.aux];
-                item += hs.nitems;
-                hub_stage[(size_t)b * p.nsub() + s] = (int)S.size();
-                S.push_back(hs);
-            }
-            if (!batch_shape(d, c.fp64))
-                return Status{6, "sub-template " + std::to_string(s) + " needs more shared memory than a CTA has"};
-            BatchStage fs{};
-            fs.kind = kStageFused;
-            fs.d = d;
-            fs.tiles_per_item = std::max(1, 1024 / d.tile_v);
-            fs.first_item = item;
-            fs.nitems = (d.ntiles + fs.tiles_per_item - 1) / fs.tiles_per_item;
-            std::vector<int> deps;
-            if (p.subs[sub.main].size > 1) deps.push_back(fused_stage[(size_t)b * p.nsub() + sub.main]);
-            if (p.subs[sub.aux].size > 1) deps.push_back(fused_stage[(size_t)b * p.nsub() + sub.aux]);
-            if (c.hubs.count > 0) deps.push_back(hub_stage[(size_t)b * p.nsub() + s]);
-            // write after read: the arena gives this table the range of tables
-            // already consumed; their consumers may still be reading it
-            if (s != 0) {
-                const int64_t lo = p.table_offset[s], hi = lo + p.table_pitch[s];
-                for (int x : p.process_order) {
-                    if (x == s) break;
-                    const int par = p.subs[x].parent;
-                    if (x == 0 || par < 0 || par >= p.nsub() || proc_index[par] >= proc_index[s]) continue;
-                    const int64_t xlo = p.table_offset[x], xhi = xlo + p.table_pitch[x];
-                    if (xlo < hi && lo < xhi) {
-                        const int dep = fused_stage[(size_t)b * p.nsub() + par];
-                        if (std::find(deps.begin(), deps.end(), dep) == deps.end()) deps.push_back(dep);
-                    }
-                }
-            }
-            if ((int)deps.size() > kBatchMaxDeps)
-                return Status{6, "sub-template " + std::to_string(s) + " needs more queue dependencies than a stage holds"};
-            for (int dep : deps) fs.deps[fs.ndeps++] = dep;
-            item += fs.nitems;
-            smem = std::max(smem, d.smem);
-            if (s == 0) bp.root_tiles = d.ntiles;
-            fused_stage[(size_t)b * p.nsub() + s] = (int)S.size();
-            S.push_back(fs);
+            void *region = c.hubs.count > 0
+                               ? (char *)bp.d_hub + hub_region * ((size_t)b * nproc + qs[b].proc_index[s])
+                               : nullptr;
+            SG_CKS(add_queue_stage(c, b, s, region, qs[b], S, item, smem));
         }
-    }
+    bp.root_tiles = qs[0].root_tiles;
     if (poison) {
         // test hook: a stage no item belongs to; the first fused stage waits on it
         BatchStage ds{};
@@ -1295,6 +1317,189 @@ Status debug_root(DeviceGraph &g, const Plan &p, uint32_t seed, int mode, int hu
         double s = 0;
         for (int32_t v = 0; v < g.V; ++v) s += root[v];
         *raw = mode == kModeReference ? s * 1.0e12 : s;
+    }
+    return Status::ok();
+}
+
+}  // namespace sg
+
+namespace sg {
+
+// ---------------------------------------------------------------------------
+// Job queues: one coloring each of jobs with different templates on one
+// graph, run as persistent work-queue launches.  Jobs are admitted in waves
+// by free device memory (each job's table arena, colors, root partials and
+// hub rows); a wave's stages go into one queue level by level (every job's
+// first sub, then every job's second, ...), each stage depending only on
+// earlier stages of its own job.  The CTA that completes a job's root stage
+// stamps %globaltimer, which gives each job's latency from the launch start.
+// ---------------------------------------------------------------------------
+Status count_jobs(DeviceGraph &g, const std::vector<const Plan *> &plans, const uint32_t *seeds,
+                  const CountOptions &o, double *raw, double *job_ms, CountStats *stats)
+{
+    const int n = (int)plans.size();
+    if (n < 1) return Status{1, "no jobs"};
+    if (!seeds || !raw) return Status{1, "null argument"};
+    if (o.mode < 0 || o.mode > 2) return Status{1, "unknown count mode"};
+    for (const Plan *p : plans)
+        if (!p) return Status{1, "null template plan"};
+    SG_CK(cudaSetDevice(g.device));
+    GraphState &gs = state_of(g);
+    Workspace &w = gs.ws;
+    const bool fp64 = o.mode == kModeFP64;
+    const size_t es = fp64 ? 8 : 4;
+    const size_t V = (size_t)g.V;
+    cudaStream_t st = g.stream;
+    const Hubs hubs = plan_hubs(g, o.exact ? 0 : o.hub_threshold);
+
+    // one context per job: its plan's device tables, its tables at arena_base
+    std::vector<RunCtx> ctx;
+    ctx.reserve(n);
+    int32_t hub_pitch = 4;
+    for (int j = 0; j < n; ++j) {
+        const Plan &p = *plans[j];
+        ctx.push_back(RunCtx{g, p, gs, nullptr, fp64, es, 0, hubs, 0, 0, o.mode, 0});
+        RunCtx &c = ctx.back();
+        SG_CKS(make_ctx_tables(g, p, gs, c.tab));
+        c.exact = o.exact != 0;
+        hub_pitch = std::max<int32_t>(hub_pitch, (int32_t)round_up(p.k, 4));
+        for (int s : p.process_order) {
+            const SubTemplate &a = p.subs[p.subs[s].aux];
+            if (a.size > 1) hub_pitch = std::max<int32_t>(hub_pitch, p.table_pitch[p.subs[s].aux]);
+        }
+    }
+    for (RunCtx &c : ctx) c.hub_pitch = hub_pitch;
+    if (hubs.count > 0) {
+        std::vector<int32_t> cs((size_t)hubs.count + 1, 0);
+        for (int h = 0; h < hubs.count; ++h) cs[h + 1] = cs[h] + (g.h_degree[h] + hubs.chunk - 1) / hubs.chunk;
+        SG_CKS(growT(&w.chunk_start, &w.chunk_start_bytes, 4 * cs.size(), st));
+        SG_CK(cudaMemcpyAsync(w.chunk_start, cs.data(), 4 * cs.size(), cudaMemcpyHostToDevice, st));
+        SG_CK(cudaStreamSynchronize(st));
+    }
+    const size_t hub_region = (size_t)hubs.total_chunks * (size_t)hub_pitch * es;
+    const long long wait_cycles = (long long)(o.wait_limit_ms > 0 ? o.wait_limit_ms : 2000) * 2000000LL;
+    const double scale = o.mode == kModeReference ? 1.0e12 : 1.0;
+    cudaEvent_t e0, e1;
+    SG_CK(cudaEventCreate(&e0));
+    SG_CK(cudaEventCreate(&e1));
+    double total_ms = 0;
+    int64_t launches = 0;
+    for (int j0 = 0; j0 < n;) {
+        // admission: jobs while their tables fit the free memory (at least one)
+        size_t free_b = 0, total_b = 0;
+        SG_CK(cudaMemGetInfo(&free_b, &total_b));
+        const size_t budget = (size_t)((double)(free_b + w.arena_bytes) * 0.85);
+        size_t arena_sum = 0, hub_sum = 0;
+        int j1 = j0;
+        while (j1 < n && j1 - j0 < 4096) {
+            const size_t a = (size_t)plans[j1]->arena_units * V * es;
+            const size_t h = hubs.count > 0 ? hub_region * plans[j1]->process_order.size() : 0;
+            const size_t per = a + h + V + 8 * (V / 8 + 2);
+            if (j1 > j0 && arena_sum + hub_sum + per > budget) break;
+            arena_sum += a;
+            hub_sum += h;
+            ++j1;
+        }
+        const int nj = j1 - j0;
+        SG_CKS(grow(&w.arena, &w.arena_bytes, std::max<size_t>(16, arena_sum), st));
+        SG_CKS(growT(&w.colors, &w.colors_bytes, std::max<size_t>(16, V * nj), st));
+        SG_CKS(growT(&w.partial, &w.partial_bytes, 8 * ((V / 8 + 2) * nj), st));
+        SG_CKS(growT(&w.windows, &w.windows_bytes, 4 * 31 * (size_t)nj, st));
+        {
+            std::vector<uint32_t> win((size_t)nj * 31);
+            for (int j = 0; j < nj; ++j) glibc_window(seeds[j0 + j], &win[(size_t)j * 31]);
+            SG_CK(cudaMemcpyAsync(w.windows, win.data(), win.size() * 4, cudaMemcpyHostToDevice, st));
+            SG_CK(cudaStreamSynchronize(st));
+        }
+        // the wave's queue
+        void *d_hub = nullptr;
+        if (hubs.count > 0) SG_CK(cudaMallocAsync(&d_hub, std::max<size_t>(16, hub_sum), st));
+        std::vector<QueueSlot> qs;
+        qs.reserve(nj);
+        std::vector<size_t> hub_off(nj, 0);
+        size_t base = 0, hoff = 0;
+        int maxlev = 0;
+        for (int j = 0; j < nj; ++j) {
+            RunCtx &c = ctx[j0 + j];
+            c.arena_base = base;
+            c.arena_per_coloring = 0;
+            base += (size_t)c.p.arena_units * V * es;
+            hub_off[j] = hoff;
+            hoff += hubs.count > 0 ? hub_region * c.p.process_order.size() : 0;
+            qs.emplace_back(c.p);
+            maxlev = std::max(maxlev, (int)c.p.process_order.size());
+        }
+        std::vector<BatchStage> S;
+        int item = 0;
+        size_t smem = (size_t)kBatchThreads * 16;
+        for (int lev = 0; lev < maxlev; ++lev)
+            for (int j = 0; j < nj; ++j) {
+                RunCtx &c = ctx[j0 + j];
+                if (lev >= (int)c.p.process_order.size()) continue;
+                const int s = c.p.process_order[lev];
+                void *region = hubs.count > 0 ? (char *)d_hub + hub_off[j] + hub_region * (size_t)qs[j].proc_index[s]
+                                              : nullptr;
+                SG_CKS(add_queue_stage(c, j, s, region, qs[j], S, item, smem));
+            }
+        std::vector<int32_t> tiles(nj);
+        for (int j = 0; j < nj; ++j) tiles[j] = qs[j].root_tiles;
+        BatchStage *d_stages = nullptr;
+        int *d_done = nullptr;
+        BatchCtl *d_ctl = nullptr;
+        unsigned long long *d_end = nullptr;
+        double *d_raw = nullptr;
+        int32_t *d_tiles = nullptr;
+        SG_CK(cudaMallocAsync(&d_stages, sizeof(BatchStage) * S.size(), st));
+        SG_CK(cudaMallocAsync(&d_done, sizeof(int) * S.size(), st));
+        SG_CK(cudaMallocAsync(&d_ctl, sizeof(BatchCtl), st));
+        SG_CK(cudaMallocAsync(&d_end, sizeof(unsigned long long) * S.size(), st));
+        SG_CK(cudaMallocAsync(&d_raw, sizeof(double) * nj, st));
+        SG_CK(cudaMallocAsync(&d_tiles, sizeof(int32_t) * nj, st));
+        SG_CK(cudaMemcpyAsync(d_stages, S.data(), sizeof(BatchStage) * S.size(), cudaMemcpyHostToDevice, st));
+        SG_CK(cudaMemcpyAsync(d_tiles, tiles.data(), sizeof(int32_t) * nj, cudaMemcpyHostToDevice, st));
+        SG_CK(cudaMemsetAsync(d_done, 0, sizeof(int) * S.size(), st));
+        SG_CK(cudaMemsetAsync(d_ctl, 0, sizeof(BatchCtl), st));
+        SG_CK(cudaMemsetAsync(d_end, 0, sizeof(unsigned long long) * S.size(), st));
+        SG_CK(cudaStreamSynchronize(st));   // `S` and `tiles` are pageable host memory
+        SG_CK(cudaEventRecord(e0, st));
+        for (int j = 0; j < nj; ++j) SG_CKS(launch_colors(ctx[j0 + j], j, j, 1, st));
+        SG_CK(launch_persistent(d_stages, (int)S.size(), item, d_done, d_ctl, wait_cycles, smem, fp64, g.sm_count, st,
+                                d_end));
+        launch_root_reduce_slots(w.partial, (int64_t)(V / 8 + 2), 0, scale, d_raw, nj, st, d_tiles);
+        SG_CK(cudaGetLastError());
+        SG_CK(cudaEventRecord(e1, st));
+        launches += nj + 2;
+        BatchCtl ctl{};
+        std::vector<unsigned long long> ends(S.size());
+        SG_CK(cudaMemcpyAsync(raw + j0, d_raw, sizeof(double) * nj, cudaMemcpyDeviceToHost, st));
+        SG_CK(cudaMemcpyAsync(&ctl, d_ctl, sizeof ctl, cudaMemcpyDeviceToHost, st));
+        SG_CK(cudaMemcpyAsync(ends.data(), d_end, sizeof(unsigned long long) * S.size(), cudaMemcpyDeviceToHost, st));
+        SG_CK(cudaStreamSynchronize(st));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        total_ms += ms;
+        for (void *q : {(void *)d_stages, (void *)d_done, (void *)d_ctl, (void *)d_end, (void *)d_raw, (void *)d_tiles,
+                        d_hub})
+            if (q) cudaFreeAsync(q, st);
+        if (ctl.error) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return Status{4, "job queue: a work item waited longer than the limit for its inputs (stage " +
+                                 std::to_string(ctl.error_stage) + ")"};
+        }
+        if (job_ms)
+            for (int j = 0; j < nj; ++j) {
+                const unsigned long long e = ends[qs[j].fused[0]];
+                job_ms[j0 + j] = e > ctl.t0 ? (double)(e - ctl.t0) * 1e-6 : 0.0;
+            }
+        j0 = j1;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (stats) {
+        stats->device_ms = total_ms;
+        stats->kernel_launches = launches;
+        stats->table_bytes = (int64_t)w.arena_bytes;
     }
     return Status::ok();
 }

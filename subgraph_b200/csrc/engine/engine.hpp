@@ -76,6 +76,13 @@ Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V,
 // Runs n_colorings colorings, writes the raw colorful counts (host).
 Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, CountStats *stats);
 
+// One coloring each of jobs of different templates on one graph (job j:
+// plans[j], seeded srand(seeds[j])), run as persistent work-queue launches
+// (waves admitted by free memory).  job_ms (optional): per-job latency from
+// the start of its wave's launch to the completion of its root stage.
+Status count_jobs(DeviceGraph &g, const std::vector<const Plan *> &plans, const uint32_t *seeds,
+                  const CountOptions &o, double *raw, double *job_ms, CountStats *stats);
+
 // Parity helpers: colors of one seed (original order), the table of sub s
 // after one coloring (column-major [L][V], original order), per-vertex root.
 Status debug_colors(DeviceGraph &g, int k, uint32_t seed, int32_t *colors);

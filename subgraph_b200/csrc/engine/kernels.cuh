@@ -63,9 +63,13 @@ void launch_fused_blk(const StageDesc &d, const FusedConfig &cfg, cudaStream_t s
 void launch_root_reduce(const double *partial, int32_t n, double scale, double *out, cudaStream_t st);
 
 // the batched form (batch.cu)
+// stage_end (optional): [nstages] %globaltimer when each stage's last item
+// completed, ctl->t0 when item 0 was claimed
 cudaError_t launch_persistent(const BatchStage *stages, int nstages, int total_items, int *done, BatchCtl *ctl,
-                              long long wait_cycles, size_t smem, bool fp64, int sm_count, cudaStream_t st);
+                              long long wait_cycles, size_t smem, bool fp64, int sm_count, cudaStream_t st,
+                              unsigned long long *stage_end = nullptr);
+// n_slot (optional): per-slot partial counts (jobs of different templates)
 void launch_root_reduce_slots(const double *partial, int64_t slot_stride, int32_t n, double scale, double *out,
-                              int nslots, cudaStream_t st);
+                              int nslots, cudaStream_t st, const int32_t *n_slot = nullptr);
 
 }  // namespace sg

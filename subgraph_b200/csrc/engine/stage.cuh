@@ -113,6 +113,7 @@ struct BatchCtl {
     int32_t error;           // set when a dependency wait ran out of time
     int32_t error_stage;
     int32_t pad;
+    unsigned long long t0;   // %globaltimer when item 0 was claimed (job latencies)
 };
 
 }  // namespace sg

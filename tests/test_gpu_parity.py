@@ -258,3 +258,33 @@ def test_fast_path_close_to_exact(golden):
     assert np.array_equal(fast, fast2)
     for a, b, r in zip(fast, exact, c.raw):
         assert rel(a, b) <= 1e-6 and rel(b, r) <= 1e-12
+
+
+def test_csr_input_path_against_oracle():
+    """CSRGraph input (CSRGraph.cpp:16-108): neighbours in edge-insertion order; the
+    aggregation sums them in that order (SpMVNaiveFull semantics), which the
+    oracle reproduces when given the CSR arrays."""
+    el = sg.rmat(11, 8, seed=6)
+    csr = sg.CSRGraph()
+    csr.createFromEdgeListFile(el.getNumVertices(), el.getNumEdges(), el.getSrcList(), el.getDstList())
+    csc = sg.CSCGraph()
+    csc.createFromEdgeListFile(el.getNumVertices(), el.getNumEdges(), el.getSrcList(), el.getDstList())
+    g_csr = csr.device_graph()
+    g_csc = csc.device_graph()
+    for tname in ("tree5", "spider7", "tree12"):
+        n, edges = TEMPLATES[tname]
+        P = O.Plan(n, edges)
+        t = sg.Graph(n, edges)
+        raw = sg.count(g_csr, t, 2, 70, exact=True)
+        for i in range(2):
+            colors = O.colors(70 + i, csr.getNumVertices(), n)
+            r_o = O.count_coloring(csr.getIndexRow(), csr.getIndexCol(), P, colors)
+            assert rel(raw[i], r_o) <= 1e-12, (tname, i, raw[i], r_o)
+        # the same graph as CSC differs only in summation order
+        raw_csc = sg.count(g_csc, t, 2, 70, exact=True)
+        for a, b in zip(raw, raw_csc):
+            assert rel(a, b) <= 1e-5, (tname, a, b)
+    cm = sg.CountMat()
+    cm.initialization(csr, None, 4, 2, 1, 0)
+    cm.set_seed(70)
+    assert cm.compute(sg.Graph(*TEMPLATES["tree5"])) > 0
