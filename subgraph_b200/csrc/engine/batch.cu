@@ -49,7 +49,7 @@ __device__ __forceinline__ void batch_fused(const StageDesc &d, int tile, unsign
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kBatchThreads, 1)
+__global__ void __launch_bounds__(kBatchThreads, 2)
     k_persistent(const BatchStage *__restrict__ stages, int nstages, int total_items, int *done, BatchCtl *ctl,
                  long long wait_cycles, unsigned long long *stage_end)
 {
@@ -148,7 +148,14 @@ cudaError_t launch_persistent(const BatchStage *stages, int nstages, int total_i
 {
     auto go = [&](auto kern) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kern<<<sm_count, kBatchThreads, smem, st>>>(stages, nstages, total_items, done, ctl, wait_cycles, stage_end);
+        // every resident CTA claims items (a claimed item only waits for items
+        // claimed earlier by running CTAs, so residency needs no guarantee)
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchThreads, smem) != cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+        kern<<<sm_count * per_sm, kBatchThreads, smem, st>>>(stages, nstages, total_items, done, ctl, wait_cycles,
+                                                               stage_end);
     };
     if (fp64) go(k_persistent<double>);
     else go(k_persistent<float>);

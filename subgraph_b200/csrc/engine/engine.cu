@@ -819,6 +819,14 @@ bool batch_shape(StageDesc &d, bool fp64)
     if (d.aux_leaf) cands = {{256, kBatchThreads, 0}, {64, kBatchThreads, 0}, {32, kBatchThreads, 0}};
     else if (heavy) cands = {{32, kBatchThreads, 1}, {32, kBatchThreads, 0}, {16, kBatchThreads, 0}, {8, kBatchThreads, 0}};
     else cands = {{32, kBatchThreads, 0}, {16, kBatchThreads, 0}, {8, kBatchThreads, 0}};
+    // first the shapes that leave room for two CTAs per SM
+    for (auto &t : cands) {
+        StageDesc e = d;
+        if (set_shape(e, fp64, t) && e.smem <= 113 * 1024) {
+            d = e;
+            return true;
+        }
+    }
     for (auto &t : cands)
         if (set_shape(d, fp64, t)) return true;
     return false;

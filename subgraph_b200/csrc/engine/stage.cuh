@@ -91,7 +91,7 @@ struct HubArgs {
 // The batched form's work queue: one entry per (coloring slot, sub-template)
 // stage, hub chunks and fused tile groups as items.
 // ---------------------------------------------------------------------------
-constexpr int kBatchThreads = 1024;   // one persistent CTA per SM
+constexpr int kBatchThreads = 512;    // persistent CTAs of 512 threads, two per SM when shared memory allows
 // producers (main, aux, hub chunks) plus the readers of earlier tables whose
 // arena range a stage overwrites; trees of up to 16 vertices need at most 9
 constexpr int kBatchMaxDeps = 12;
