@@ -156,7 +156,7 @@ sg_status sg_count(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw, s
  * coloring of plans[j] seeded srand(seeds[j]) into raw[j].  The jobs run as
  * persistent work-queue launches (all their sub-template stages in one queue,
  * waves admitted by free device memory).  From opts: mode, hub_threshold,
- * exact, wait_limit_ms.  job_ms (optional, n_jobs): each job's latency from
+ * exact, wait_limit_ms, no_autotune.  job_ms (optional, n_jobs): each job's latency from
  * the start of its wave's launch to the end of its last stage.  The reference
  * runs one template per CountMat::compute (CountMat.cpp:79-266); this is the
  * batched mixed-template form with no single counterpart there. */

@@ -352,6 +352,7 @@ sg_status sg_count_jobs(sg_graph g, int32_t n_jobs, const sg_plan *plans, const 
     co.hub_threshold = o->hub_threshold;
     co.exact = o->exact ? 1 : 0;
     co.wait_limit_ms = o->wait_limit_ms;
+    co.autotune = o->no_autotune ? 0 : 1;
     sg::CountStats cs;
     sg_status st = from(sg::count_jobs(*g->g, ps, seeds, co, raw, job_ms, &cs));
     if (st) return st;

@@ -812,14 +812,19 @@ Status upload_windows(RunCtx &c, uint32_t seed_base, int n)
 }
 
 // Tile shape of a stage in the persistent kernel (1024 threads, one CTA per SM).
-bool batch_shape(StageDesc &d, bool fp64)
+// Tile shape of a stage in the persistent kernel (kBatchThreads threads, up
+// to two CTAs per SM): the candidates that leave room for two CTAs first.
+std::vector<TileShape> batch_candidates(const StageDesc &d)
 {
     const bool heavy = !d.main_leaf && !d.is_root && (int64_t)d.S * d.L_s >= 512;
-    std::vector<TileShape> cands;
-    if (d.aux_leaf) cands = {{256, kBatchThreads, 0}, {64, kBatchThreads, 0}, {32, kBatchThreads, 0}};
-    else if (heavy) cands = {{32, kBatchThreads, 1}, {32, kBatchThreads, 0}, {16, kBatchThreads, 0}, {8, kBatchThreads, 0}};
-    else cands = {{32, kBatchThreads, 0}, {16, kBatchThreads, 0}, {8, kBatchThreads, 0}};
-    // first the shapes that leave room for two CTAs per SM
+    if (d.aux_leaf) return {{256, kBatchThreads, 0}, {128, kBatchThreads, 0}, {64, kBatchThreads, 0}, {32, kBatchThreads, 0}};
+    if (heavy) return {{32, kBatchThreads, 1}, {32, kBatchThreads, 0}, {16, kBatchThreads, 0}, {8, kBatchThreads, 0}};
+    return {{32, kBatchThreads, 0}, {16, kBatchThreads, 0}, {8, kBatchThreads, 0}};
+}
+
+bool batch_shape(StageDesc &d, bool fp64)
+{
+    const std::vector<TileShape> cands = batch_candidates(d);
     for (auto &t : cands) {
         StageDesc e = d;
         if (set_shape(e, fp64, t) && e.smem <= 113 * 1024) {
@@ -830,6 +835,77 @@ bool batch_shape(StageDesc &d, bool fp64)
     for (auto &t : cands)
         if (set_shape(d, fp64, t)) return true;
     return false;
+}
+
+// The persistent kernel runs the tile body of the plain kernel of the same
+// thread count, so a stage's queue shape is chosen by timing the candidates
+// (those under 113 KB of shared memory when any fit) through that kernel on
+// the stage's own buffers: trial launches read whatever the inputs hold and
+// write the stage's output, which the queue rewrites.  Cached process-wide by
+// graph signature and stage shape.
+std::map<std::string, TileShape> g_batch_tuned;
+
+Status queue_shape(RunCtx &c, StageDesc &d)
+{
+    const std::string key = graph_sig(c.g) + shape_key(d, c.fp64, c.hubs.count) + (d.aoff ? "/pk" : "/ex") + "/queue";
+    {
+        std::lock_guard<std::mutex> lk(g_state_mu);
+        auto it = g_batch_tuned.find(key);
+        if (it != g_batch_tuned.end() && set_shape(d, c.fp64, it->second)) return Status::ok();
+    }
+    if (!c.autotune) {
+        if (!batch_shape(d, c.fp64)) return Status{6, "a sub-template needs more shared memory than a CTA has"};
+        return Status::ok();
+    }
+    std::vector<TileShape> fit, all;
+    for (const TileShape &t : batch_candidates(d)) {
+        StageDesc e = d;
+        if (!set_shape(e, c.fp64, t)) continue;
+        all.push_back(t);
+        if (e.smem <= 113 * 1024) fit.push_back(t);
+    }
+    const std::vector<TileShape> &cands = fit.empty() ? all : fit;
+    if (cands.empty()) return Status{6, "a sub-template needs more shared memory than a CTA has"};
+    cudaStream_t st = c.g.stream;
+    // the queue is built before its colorings' colors exist, and colors are
+    // indices (histogram rows, rem lookups): give the trial launches valid
+    // ones (0 < k); the queue's own color launch overwrites them
+    SG_CK(cudaMemsetAsync(const_cast<uint8_t *>(d.color), 0, (size_t)c.g.V * (size_t)d.cstride, st));
+    cudaEvent_t e0, e1;
+    SG_CK(cudaEventCreate(&e0));
+    SG_CK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    TileShape pick = cands.front();
+    for (const TileShape &t : cands) {
+        StageDesc e = d;
+        set_shape(e, c.fp64, t);
+        FusedConfig cfg;
+        cfg.tile_v = e.tile_v;
+        cfg.q = e.gather_q;
+        cfg.smem = e.smem;
+        cfg.grid = c.g.sm_count;
+        launch_fused(e, c.fp64, cfg, st);
+        float ms = 1e30f;
+        for (int rep = 0; rep < 2; ++rep) {
+            SG_CK(cudaEventRecord(e0, st));
+            launch_fused(e, c.fp64, cfg, st);
+            SG_CK(cudaEventRecord(e1, st));
+            SG_CK(cudaEventSynchronize(e1));
+            SG_CK(cudaGetLastError());
+            float tt = 0;
+            cudaEventElapsedTime(&tt, e0, e1);
+            ms = std::min(ms, tt);
+        }
+        if (ms < best) { best = ms; pick = t; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    {
+        std::lock_guard<std::mutex> lk(g_state_mu);
+        g_batch_tuned[key] = pick;
+    }
+    set_shape(d, c.fp64, pick);
+    return Status::ok();
 }
 
 // The queue stages of one coloring slot of context c: per sub (in processing
@@ -862,8 +938,7 @@ Status add_queue_stage(RunCtx &c, int slot, int s, void *hub_region, QueueSlot &
         q.hub[s] = (int)S.size();
         S.push_back(hs);
     }
-    if (!batch_shape(d, c.fp64))
-        return Status{6, "sub-template " + std::to_string(s) + " needs more shared memory than a CTA has"};
+    SG_CKS(queue_shape(c, d));
     BatchStage fs{};
     fs.kind = kStageFused;
     fs.d = d;
@@ -1370,6 +1445,7 @@ Status count_jobs(DeviceGraph &g, const std::vector<const Plan *> &plans, const 
         RunCtx &c = ctx.back();
         SG_CKS(make_ctx_tables(g, p, gs, c.tab));
         c.exact = o.exact != 0;
+        c.autotune = o.autotune != 0;
         hub_pitch = std::max<int32_t>(hub_pitch, (int32_t)round_up(p.k, 4));
         for (int s : p.process_order) {
             const SubTemplate &a = p.subs[p.subs[s].aux];
