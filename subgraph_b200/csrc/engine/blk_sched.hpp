@@ -97,9 +97,11 @@ template <int N, int P> struct Sched {
 // The shapes with a blocked kernel: (N, P) with P >= 2 (a one-hot main has its
 // own path), N <= 11, at most 64 held values.  Index 0 means "no blocked
 // path"; shape ids are 1 + the position in this list.
-#define SG_BLK_SHAPES(X) \
-    X(3, 2) X(4, 2) X(4, 3) X(5, 2) X(5, 3) X(5, 4) X(6, 2) X(6, 3) X(6, 4) X(6, 5) X(7, 2) X(7, 3) X(7, 4) \
-    X(7, 5) X(7, 6) X(8, 2) X(8, 6) X(8, 7) X(9, 2) X(9, 7) X(9, 8) X(10, 2) X(10, 8) X(10, 9) X(11, 10)
+#define SG_BLK_SHAPES_A(X) X(3, 2) X(4, 2) X(4, 3) X(5, 2) X(5, 3) X(5, 4) X(6, 2) X(6, 3)
+#define SG_BLK_SHAPES_B(X) X(6, 4) X(6, 5) X(7, 2) X(7, 3) X(7, 4) X(7, 5)
+#define SG_BLK_SHAPES_C(X) X(7, 6) X(8, 2) X(8, 6) X(8, 7) X(9, 2) X(9, 7)
+#define SG_BLK_SHAPES_D(X) X(9, 8) X(10, 2) X(10, 8) X(10, 9) X(11, 10)
+#define SG_BLK_SHAPES(X) SG_BLK_SHAPES_A(X) SG_BLK_SHAPES_B(X) SG_BLK_SHAPES_C(X) SG_BLK_SHAPES_D(X)
 
 // Runtime view of one shape's schedule (host planner).
 struct View {

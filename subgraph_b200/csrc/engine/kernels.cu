@@ -277,19 +277,9 @@ void launch_fused(const StageDesc &d, bool fp64, const FusedConfig &cfg, cudaStr
     }
 }
 
-// Wide rows (more than 128 16-byte column chunks) get 1024-thread CTAs, so
-// that every chunk of a hub's neighbour list is still summed by several
-// neighbour lanes; narrow rows and colour counts use 256 threads.
 void launch_hub(const HubArgs &h, bool fp64, int sm_count, cudaStream_t st)
 {
     if (h.hub_count == 0 || h.total_chunks == 0) return;
-    const int nchunk = h.k_leaf ? 0 : (h.L_a + (fp64 ? 1 : 3)) / (fp64 ? 2 : 4);
-    if (nchunk > 128) {
-        const int grid = std::max(1, std::min(h.total_chunks, sm_count * 2));
-        if (fp64) k_hub<double, 1024><<<grid, 1024, 0, st>>>(h);
-        else k_hub<float, 1024><<<grid, 1024, 0, st>>>(h);
-        return;
-    }
     const int grid = std::max(1, std::min(h.total_chunks, sm_count * 8));
     if (fp64) k_hub<double, 256><<<grid, 256, 0, st>>>(h);
     else k_hub<float, 256><<<grid, 256, 0, st>>>(h);

@@ -129,7 +129,7 @@ __device__ __forceinline__ unsigned long long add2_rn(unsigned long long a, unsi
 //      per vertex, reduced over the tile in a fixed order.
 // The aggregate never leaves the chip.
 // ---------------------------------------------------------------------------
-template <typename T, int NT, int Q, bool PK = false, bool COH = false, bool BLK = false>
+template <typename T, int NT, int Q, bool PK = false, bool COH = false, bool BLK = false, int BN = 0, int BP = 0>
 __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigned char *smem_raw)
 {
     using CT = Chunk<T>;
@@ -367,7 +367,8 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
         if constexpr (BLK && sizeof(T) == 4 && !PK) {
             T *outp = reinterpret_cast<T *>(d.out);
             const int P = d.out_pitch, W = d.out_w;
-            blk::ema_blocked(d, agg_s, main_s, out_s, RS, TVP, TV, warp, NW, lane);
+            if constexpr (BN > 0) blk::ema_blocks<BN, BP>(d, agg_s, main_s, out_s, RS, TVP, TV, warp, NW, lane);
+            else blk::ema_blocked(d, agg_s, main_s, out_s, RS, TVP, TV, warp, NW, lane);
             __syncthreads();
             const FastDiv fd = fast_div(W, tv * W);
             for (int idx = tid; idx < tv * W; idx += NT) {
@@ -563,9 +564,13 @@ __device__ __forceinline__ void hub_item(const HubArgs &h, int item, unsigned ch
         uint32_t *cnt = reinterpret_cast<uint32_t *>(smem_raw);
         for (int i = threadIdx.x; i < nk; i += NT) cnt[i] = 0;
         __syncthreads();
-        for (int e = beg + (int)threadIdx.x; e < end; e += NT) {
-            const uint8_t *cp = h.color + (size_t)__ldg(h.adj + e) * h.cstride;
-            for (int b = 0; b < h.nb; ++b) atomicAdd(&cnt[b * h.k_leaf + __ldg(cp + b)], 1u);
+        if (h.nb == 1 && h.cstride == 1) {
+            for (int e = beg + (int)threadIdx.x; e < end; e += NT) atomicAdd(&cnt[__ldg(h.color + __ldg(h.adj + e))], 1u);
+        } else {
+            for (int e = beg + (int)threadIdx.x; e < end; e += NT) {
+                const uint8_t *cp = h.color + (size_t)__ldg(h.adj + e) * h.cstride;
+                for (int b = 0; b < h.nb; ++b) atomicAdd(&cnt[b * h.k_leaf + __ldg(cp + b)], 1u);
+            }
         }
         __syncthreads();
         for (int i = threadIdx.x; i < nk; i += NT) prow[i] = (T)cnt[i];
