@@ -156,74 +156,37 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
 
     // ---- A: aggregation ------------------------------------------------------
     if (d.aux_leaf) {
-        // per-color neighbour counts (row b*k + c for coloring b), one thread
-        // per vertex (exact integers)
+        // per-color neighbour counts (row b*k + c for coloring b): one thread per
+        // (vertex, coloring), each owning its k counters (exact integers, no
+        // atomics), neighbours in predicated batches of 8 with their loads in
+        // flight together
         const int nk = nbc * d.k;
-        const bool words = (nbc & 3) == 0 && (d.cstride & 3) == 0 &&   // 4 colorings per aligned load
-                           (reinterpret_cast<uintptr_t>(d.color) & 3) == 0;
-        for (int vi = tid; vi < tv; vi += NT) {
+        for (int vi = tid; vi < tv; vi += NT)
             for (int c = 0; c < nk; ++c) agg_s[c * RS + vi] = T(0);
+        __syncthreads();
+        for (int idx = tid; idx < nbc * tv; idx += NT) {
+            const int b = idx / tv, vi = idx - b * tv;
             const int v = v0 + vi;
+            T *cnt = agg_s + (size_t)b * d.k * RS + vi;
             if (v < d.hub_count) {
-                const T *p = reinterpret_cast<const T *>(d.hub_partial);
+                const T *p = reinterpret_cast<const T *>(d.hub_partial) + b * d.k;
                 const int c0 = __ldg(d.hub_chunk_start + v), c1 = __ldg(d.hub_chunk_start + v + 1);
                 for (int ch = c0; ch < c1; ++ch)
-                    for (int c = 0; c < nk; ++c)
-                        agg_s[c * RS + vi] = add_rn(agg_s[c * RS + vi], ld_tab<COH>(p + (size_t)ch * d.hub_pitch + c));
+                    for (int c = 0; c < d.k; ++c)
+                        cnt[c * RS] = add_rn(cnt[c * RS], ld_tab<COH>(p + (size_t)ch * d.hub_pitch + c));
                 continue;
             }
             const int beg = __ldg(d.off + v), end = __ldg(d.off + v + 1);
-            if (nbc == 1) {
-                // batches of 8 neighbours, the last one predicated: every batch
-                // has its loads in flight together
-                for (int e = beg; e < end; e += 8) {
-                    int nb[8], cl[8];
+            const uint8_t *col = d.color + b;
+            for (int e = beg; e < end; e += 8) {
+                int nb[8], cl[8];
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) nb[u] = e + u < end ? __ldg(d.adj + e + u) : -1;
+                for (int u = 0; u < 8; ++u) nb[u] = e + u < end ? __ldg(d.adj + e + u) : -1;
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) cl[u] = nb[u] >= 0 ? (int)__ldg(d.color + (size_t)nb[u] * d.cstride) : -1;
+                for (int u = 0; u < 8; ++u) cl[u] = nb[u] >= 0 ? (int)__ldg(col + (size_t)nb[u] * d.cstride) : -1;
 #pragma unroll
-                    for (int u = 0; u < 8; ++u)
-                        if (cl[u] >= 0) agg_s[cl[u] * RS + vi] += T(1);
-                }
-            } else if (words) {
-                // a neighbour's colors are nbc/4 32-bit words, taken 4 words
-                // (16 colorings) at a time for 4 neighbours at once
-                const int nw = nbc >> 2;
-                for (int e = beg; e < end; e += 4) {
-                    int nb[4];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) nb[u] = e + u < end ? __ldg(d.adj + e + u) : -1;
-                    for (int w0 = 0; w0 < nw; w0 += 4) {
-                        uint32_t cw[4][4];
-#pragma unroll
-                        for (int u = 0; u < 4; ++u)
-#pragma unroll
-                            for (int w = 0; w < 4; ++w)
-                                cw[u][w] = (nb[u] >= 0 && w0 + w < nw)
-                                               ? __ldg(reinterpret_cast<const uint32_t *>(d.color + (size_t)nb[u] * d.cstride) +
-                                                       w0 + w)
-                                               : 0u;
-#pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            if (nb[u] < 0) continue;
-#pragma unroll
-                            for (int w = 0; w < 4; ++w) {
-                                if (w0 + w >= nw) continue;
-#pragma unroll
-                                for (int i = 0; i < 4; ++i) {
-                                    const int c = (int)((cw[u][w] >> (8 * i)) & 0xffu);
-                                    agg_s[((4 * (w0 + w) + i) * d.k + c) * RS + vi] += T(1);
-                                }
-                            }
-                        }
-                    }
-                }
-            } else {
-                for (int e = beg; e < end; ++e) {
-                    const uint8_t *cp = d.color + (size_t)__ldg(d.adj + e) * d.cstride;
-                    for (int b = 0; b < nbc; ++b) agg_s[(b * d.k + __ldg(cp + b)) * RS + vi] += T(1);
-                }
+                for (int u = 0; u < 8; ++u)
+                    if (cl[u] >= 0) cnt[cl[u] * RS] += T(1);
             }
         }
     } else {
