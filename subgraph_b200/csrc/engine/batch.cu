@@ -55,7 +55,9 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ BatchStage st;
-    __shared__ int s_item, s_stage, s_skip;
+    __shared__ int s_item, s_stage, s_skip, s_cur;
+    if (threadIdx.x == 0) s_cur = -1;   // the stage whose descriptor is in `st`
+    __syncthreads();
     for (;;) {
         if (threadIdx.x == 0) {
             s_item = atomicAdd(&ctl->next_item, 1);
@@ -88,16 +90,18 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
             s_skip = ld_acquire(&ctl->error);
         }
         __syncthreads();
-        {   // the stage descriptor into shared memory
+        if (s_stage != s_cur) {   // the stage descriptor into shared memory, when it changes
             const int *src = reinterpret_cast<const int *>(stages + s_stage);
             int *dst = reinterpret_cast<int *>(&st);
             for (int i = threadIdx.x; i < (int)(sizeof(BatchStage) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
         }
         __syncthreads();
+        if (threadIdx.x == 0) s_cur = s_stage;   // read again only after the barriers below
         if (!s_skip) {
             const int local = item - st.first_item;
             if (st.kind == kStageHub) {
-                hub_item<T, kBatchThreads, true>(st.h, local, smem_raw);
+                const int c1 = min((local + 1) * kHubItemChunks, st.h.total_chunks);
+                for (int ch = local * kHubItemChunks; ch < c1; ++ch) hub_item<T, kBatchThreads, true>(st.h, ch, smem_raw);
             } else {
                 const int t0 = local * st.tiles_per_item;
                 const int t1 = min(t0 + st.tiles_per_item, st.d.ntiles);

@@ -932,7 +932,7 @@ Status add_queue_stage(RunCtx &c, int slot, int s, void *hub_region, QueueSlot &
         hs.kind = kStageHub;
         hs.h = make_hub(c, d, hub_region);
         hs.first_item = item;
-        hs.nitems = c.hubs.total_chunks;
+        hs.nitems = (c.hubs.total_chunks + kHubItemChunks - 1) / kHubItemChunks;
         if (p.subs[sub.aux].size > 1) hs.deps[hs.ndeps++] = q.fused[sub.aux];
         item += hs.nitems;
         q.hub[s] = (int)S.size();

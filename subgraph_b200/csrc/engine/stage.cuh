@@ -96,6 +96,7 @@ constexpr int kBatchThreads = 512;    // persistent CTAs of 512 threads, two per
 // arena range a stage overwrites; trees of up to 16 vertices need at most 9
 constexpr int kBatchMaxDeps = 12;
 constexpr int kStageHub = 0, kStageFused = 1;
+constexpr int kHubItemChunks = 8;     // hub neighbour chunks per queue item
 
 struct BatchStage {
     int32_t kind;            // kStageHub or kStageFused
