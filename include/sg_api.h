@@ -144,6 +144,12 @@ typedef struct {
                                 read once, the output written once, the adjacency once */
     double fused_gather_bytes; /* neighbour-row bytes the aggregation reads (4*nnz*L_a) */
     double hub_ms;           /* summed time of the hub aggregation launches */
+    /* with profile != 0: the sub-template whose fused launches took the most
+       time (the dominant kernel), its launches, summed time and compulsory bytes */
+    int32_t top_sub;
+    int64_t top_launches;
+    double top_ms;
+    double top_alg_bytes;
 } sg_count_stats;
 
 void sg_count_opts_default(sg_count_opts *o);

@@ -55,7 +55,8 @@ class CountOpts(ctypes.Structure):
 class CountStats(ctypes.Structure):
     _fields_ = [("device_ms", ctypes.c_double), ("kernel_launches", ctypes.c_int64), ("table_bytes", ctypes.c_int64),
                 ("fused_ms", ctypes.c_double), ("fused_launches", ctypes.c_int64), ("fused_alg_bytes", ctypes.c_double),
-                ("fused_gather_bytes", ctypes.c_double), ("hub_ms", ctypes.c_double)]
+                ("fused_gather_bytes", ctypes.c_double), ("hub_ms", ctypes.c_double), ("top_sub", ctypes.c_int32),
+                ("top_launches", ctypes.c_int64), ("top_ms", ctypes.c_double), ("top_alg_bytes", ctypes.c_double)]
 
 
 _lib = None

@@ -331,6 +331,10 @@ sg_status sg_count(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw, s
         stats->fused_alg_bytes = cs.fused_alg_bytes;
         stats->fused_gather_bytes = cs.fused_gather_bytes;
         stats->hub_ms = cs.hub_ms;
+        stats->top_sub = cs.top_sub;
+        stats->top_launches = cs.top_launches;
+        stats->top_ms = cs.top_ms;
+        stats->top_alg_bytes = cs.top_alg_bytes;
     }
     return SG_OK;
     SG_GUARD_END

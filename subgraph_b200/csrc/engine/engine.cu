@@ -530,6 +530,7 @@ struct RunCtx {
     size_t arena_base = 0;   // byte offset of this context's tables in the arena (job queues)
     bool exact = false;      // no fused products (packed eMA), no hub chunks
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> fused_ev, hub_ev;
+    std::vector<std::pair<int, double>> fused_sub;   // per fused launch: sub, compulsory bytes
     double fused_alg_bytes = 0, fused_gather_bytes = 0;
 };
 
@@ -554,6 +555,31 @@ double ev_sum(std::vector<std::pair<cudaEvent_t, cudaEvent_t>> &v)
     }
     v.clear();
     return t;
+}
+
+// The sub whose fused launches took the most summed time (profile mode):
+// its launches, time and compulsory bytes.  Reads the events before ev_sum
+// releases them.
+void top_stage(RunCtx &c, CountStats *stats)
+{
+    std::map<int, std::pair<double, double>> per;   // sub -> (ms, bytes)
+    std::map<int, int64_t> n;
+    for (size_t i = 0; i < c.fused_ev.size() && i < c.fused_sub.size(); ++i) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c.fused_ev[i].first, c.fused_ev[i].second);
+        auto &e = per[c.fused_sub[i].first];
+        e.first += ms;
+        e.second += c.fused_sub[i].second;
+        ++n[c.fused_sub[i].first];
+    }
+    stats->top_sub = -1;
+    for (auto &kv : per)
+        if (kv.second.first > stats->top_ms) {
+            stats->top_sub = kv.first;
+            stats->top_ms = kv.second.first;
+            stats->top_alg_bytes = kv.second.second;
+            stats->top_launches = n[kv.first];
+        }
 }
 
 Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
@@ -762,7 +788,9 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
         // the adjacency read once (offsets + neighbour ids)
         const double V = (double)g.V, nb = (double)d.nb;
         const double lm = d.main_leaf ? 1.0 : (double)d.L_m, la = d.aux_leaf ? 1.0 : (double)d.L_a;
-        c.fused_alg_bytes += nb * (double)c.es * V * (lm + la + (s ? (double)d.L_s : 0.0)) + 4.0 * (V + 1 + (double)g.nnz);
+        const double alg = nb * (double)c.es * V * (lm + la + (s ? (double)d.L_s : 0.0)) + 4.0 * (V + 1 + (double)g.nnz);
+        c.fused_alg_bytes += alg;
+        c.fused_sub.push_back({s, alg});
         c.fused_gather_bytes += nb * (double)c.es * (double)g.nnz * (d.aux_leaf ? 0.25 : (double)d.L_a);
     }
     c.launches += 1;
@@ -1245,6 +1273,7 @@ Status count_grouped(RunCtx &c, const CountOptions &o, double *raw, CountStats *
         stats->kernel_launches = c.launches;
         stats->table_bytes = (int64_t)(c.arena_per_coloring * B);
         stats->fused_launches = (int64_t)c.fused_ev.size();
+        top_stage(c, stats);
         stats->fused_ms = ev_sum(c.fused_ev);
         stats->hub_ms = ev_sum(c.hub_ev);
         stats->fused_alg_bytes = c.fused_alg_bytes;
@@ -1298,6 +1327,7 @@ Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, 
         stats->kernel_launches = c.launches;
         stats->table_bytes = (int64_t)(c.arena_per_coloring * slots);
         stats->fused_launches = (int64_t)c.fused_ev.size();
+        top_stage(c, stats);
         stats->fused_ms = ev_sum(c.fused_ev);
         stats->hub_ms = ev_sum(c.hub_ev);
         stats->fused_alg_bytes = c.fused_alg_bytes;

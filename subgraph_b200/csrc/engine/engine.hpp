@@ -68,6 +68,9 @@ struct CountStats {
     double fused_alg_bytes = 0; // compulsory bytes of the fused launches
     double fused_gather_bytes = 0;
     double hub_ms = 0;
+    int32_t top_sub = -1;       // profile: the sub whose fused launches took the most time
+    int64_t top_launches = 0;
+    double top_ms = 0, top_alg_bytes = 0;
 };
 
 Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V, int64_t nnz, int device,
