@@ -101,6 +101,29 @@ sg_status sg_plan_sub_edges(sg_plan p, int32_t s, int32_t *n, int32_t *src, int3
  * 686-735) or a CSR (indexRow, indexCol) for the CSRGraph path. */
 sg_status sg_graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V, int64_t nnz,
                           int32_t device, sg_graph *out);
+
+/* Input preparation on the GPU, each ending in a graph handle without a host
+ * copy of the adjacency:
+ *  - sg_graph_create_edges: CSC of the symmetrised adjacency of host edge
+ *    arrays built on the GPU (CSCGraph::createFromEdgeListFile,
+ *    CSCGraph.hpp:95-178: both directions, duplicates and self loops kept,
+ *    rows of every column ascending);
+ *  - sg_graph_create_text: an edge-list text file ("V\nE\nu v\n...",
+ *    EdgeList::readfromEdgeList, EdgeList.cpp:34-116) parsed on the GPU, hole
+ *    removal included; every edge line must contain a space (the field before
+ *    it is u, the rest of the line v), other lines are an error;
+ *  - sg_graph_create_rmat: an R-MAT graph (initiator a, b, c, 1-a-b-c,
+ *    edge_factor * 2^scale draws) generated, deduplicated and built on the
+ *    GPU from counter-based SplitMix64 draws (the same seed gives the same
+ *    graph; a different stream from sg_rmat_generate's);
+ *  - sg_graph_download_csc: the CSC of a graph in original vertex order
+ *    (offsets[V+1], neighbors[nnz]), e.g. to write graph.data. */
+sg_status sg_graph_create_edges(int32_t V, const int32_t *src, const int32_t *dst, int64_t E, int32_t device,
+                                sg_graph *out);
+sg_status sg_graph_create_text(const char *path, int32_t device, sg_graph *out);
+sg_status sg_graph_create_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, uint64_t seed,
+                               int32_t device, sg_graph *out);
+sg_status sg_graph_download_csc(sg_graph g, int32_t *offsets, int32_t *neighbors);
 void sg_graph_destroy(sg_graph g);
 sg_status sg_graph_info(sg_graph g, int32_t *V, int64_t *nnz, int32_t *max_degree);
 

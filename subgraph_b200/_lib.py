@@ -30,7 +30,8 @@ EXPORTS = [
     "sg_graph_data_write", "sg_graph_data_read", "sg_rmat_generate",
     "sg_plan_create", "sg_plan_read", "sg_plan_destroy", "sg_plan_info", "sg_plan_sub",
     "sg_plan_tables", "sg_plan_automorphisms", "sg_plan_sub_edges",
-    "sg_graph_create", "sg_graph_destroy", "sg_graph_info",
+    "sg_graph_create", "sg_graph_destroy", "sg_graph_info", "sg_graph_create_edges", "sg_graph_create_text",
+    "sg_graph_create_rmat", "sg_graph_download_csc",
     "sg_count_opts_default", "sg_count", "sg_count_jobs", "sg_estimate",
     "sg_colors", "sg_debug_sub_table", "sg_debug_root", "sg_colors_noalloc",
     "sg_countmat_create", "sg_countmat_destroy", "sg_countmat_initialization",
@@ -96,6 +97,11 @@ def lib() -> ctypes.CDLL:
         "sg_graph_create": ([vp, vp, i32, i64, i32, pp], i32),
         "sg_graph_destroy": ([vp], None),
         "sg_graph_info": ([vp, P(i32), P(i64), P(i32)], i32),
+        "sg_graph_create_edges": ([i32, vp, vp, i64, i32, pp], i32),
+        "sg_graph_create_text": ([ctypes.c_char_p, i32, pp], i32),
+        "sg_graph_create_rmat": ([i32, i32, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_uint64, i32,
+                                  pp], i32),
+        "sg_graph_download_csc": ([vp, vp, vp], i32),
         "sg_count_opts_default": ([P(CountOpts)], None),
         "sg_count": ([vp, vp, P(CountOpts), vp, P(CountStats)], i32),
         "sg_count_jobs": ([vp, i32, vp, vp, P(CountOpts), vp, vp, P(CountStats)], i32),

@@ -230,6 +230,49 @@ class DeviceGraph:
         self.V = len(off) - 1
         self.nnz = len(nbr)
 
+    @classmethod
+    def _wrap(cls, h):
+        self = cls.__new__(cls)
+        self._h = h
+        V, nnz = ctypes.c_int32(), ctypes.c_int64()
+        check(lib().sg_graph_info(h, ctypes.byref(V), ctypes.byref(nnz), None))
+        self.V, self.nnz = V.value, nnz.value
+        return self
+
+    @classmethod
+    def from_edges(cls, V: int, src, dst, device: int = 0) -> "DeviceGraph":
+        """CSC of the symmetrised edge list built on the GPU (CSCGraph::createFromEdgeListFile)."""
+        s = np.ascontiguousarray(src, np.int32)
+        d = np.ascontiguousarray(dst, np.int32)
+        if len(s) != len(d):
+            raise ValueError("src and dst differ in length")
+        h = ctypes.c_void_p()
+        check(lib().sg_graph_create_edges(V, _p(s), _p(d), len(s), device, ctypes.byref(h)))
+        return cls._wrap(h)
+
+    @classmethod
+    def from_edge_list_file(cls, path: str, device: int = 0) -> "DeviceGraph":
+        """An edge-list text file ("V\\nE\\nu v\\n...") parsed and built on the GPU."""
+        h = ctypes.c_void_p()
+        check(lib().sg_graph_create_text(path.encode(), device, ctypes.byref(h)))
+        return cls._wrap(h)
+
+    @classmethod
+    def from_rmat(cls, scale: int, edge_factor: int, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+                  seed: int = 1, device: int = 0) -> "DeviceGraph":
+        """An R-MAT graph generated, deduplicated and built on the GPU."""
+        h = ctypes.c_void_p()
+        check(lib().sg_graph_create_rmat(scale, edge_factor, a, b, c, seed & 0xFFFFFFFFFFFFFFFF, device,
+                                         ctypes.byref(h)))
+        return cls._wrap(h)
+
+    def csc(self):
+        """(offsets, neighbors) of the graph in original vertex order."""
+        off = np.zeros(self.V + 1, np.int32)
+        nbr = np.zeros(max(self.nnz, 1), np.int32)
+        check(lib().sg_graph_download_csc(self._h, _p(off), _p(nbr)))
+        return off, nbr[: self.nnz]
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:

@@ -282,6 +282,52 @@ sg_status sg_graph_create(const int32_t *offsets, const int32_t *neighbors, int3
     SG_GUARD_END
 }
 
+sg_status sg_graph_create_edges(int32_t V, const int32_t *src, const int32_t *dst, int64_t E, int32_t device,
+                                sg_graph *out)
+{
+    SG_GUARD_BEGIN
+    if (!out) return fail(SG_ERR_INVALID, "null argument");
+    auto h = std::make_unique<sg_graph_s>();
+    sg_status st = from(sg::graph_from_edges(V, src, dst, E, device, h->g));
+    if (st) return st;
+    *out = h.release();
+    return SG_OK;
+    SG_GUARD_END
+}
+
+sg_status sg_graph_create_text(const char *path, int32_t device, sg_graph *out)
+{
+    SG_GUARD_BEGIN
+    if (!out || !path) return fail(SG_ERR_INVALID, "null argument");
+    auto h = std::make_unique<sg_graph_s>();
+    sg_status st = from(sg::graph_from_text(path, device, h->g));
+    if (st) return st;
+    *out = h.release();
+    return SG_OK;
+    SG_GUARD_END
+}
+
+sg_status sg_graph_create_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, uint64_t seed,
+                               int32_t device, sg_graph *out)
+{
+    SG_GUARD_BEGIN
+    if (!out) return fail(SG_ERR_INVALID, "null argument");
+    auto h = std::make_unique<sg_graph_s>();
+    sg_status st = from(sg::graph_from_rmat(scale, edge_factor, a, b, c, seed, device, h->g));
+    if (st) return st;
+    *out = h.release();
+    return SG_OK;
+    SG_GUARD_END
+}
+
+sg_status sg_graph_download_csc(sg_graph g, int32_t *offsets, int32_t *neighbors)
+{
+    SG_GUARD_BEGIN
+    if (!g) return fail(SG_ERR_INVALID, "null graph");
+    return from(sg::graph_download_csc(*g->g, offsets, neighbors));
+    SG_GUARD_END
+}
+
 void sg_graph_destroy(sg_graph g) { delete g; }
 
 sg_status sg_graph_info(sg_graph g, int32_t *V, int64_t *nnz, int32_t *max_degree)

@@ -418,14 +418,8 @@ DeviceGraph::~DeviceGraph()
     cudaSetDevice(prev);
 }
 
-Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V, int64_t nnz, int device,
-                    std::unique_ptr<DeviceGraph> &out)
+Status new_device_graph(int device, int32_t V, int64_t nnz, std::unique_ptr<DeviceGraph> &out)
 {
-    if (V < 0 || nnz < 0 || nnz > 0x7fffffffLL) return Status{1, "vertex or entry count out of range"};
-    if (!offsets || (nnz > 0 && !neighbors)) return Status{1, "null graph array"};
-    if (offsets[0] != 0 || offsets[V] != nnz) return Status{1, "offsets[0] must be 0 and offsets[V] must equal nnz"};
-    for (int32_t v = 0; v < V; ++v)
-        if (offsets[v + 1] < offsets[v]) return Status{1, "offsets are not monotone"};
     int ndev = 0;
     SG_CK(cudaGetDeviceCount(&ndev));
     if (device < 0 || device >= ndev) return Status{1, "no CUDA device " + std::to_string(device)};
@@ -437,10 +431,21 @@ Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V,
     SG_CK(cudaDeviceGetAttribute(&g->sm_count, cudaDevAttrMultiProcessorCount, device));
     SG_CK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
     keep_pool_memory(device);
-    // degree order: counting sort by degree, descending, stable in the id
-    std::vector<int32_t> deg(V);
+    out = std::move(g);
+    return Status::ok();
+}
+
+// The common tail of every graph upload: the degree order (counting sort by
+// descending degree, stable in the id, on the V host degrees), the relabelled
+// adjacency (k_remap from the original-order device arrays, which this frees)
+// and the coloring jump-ahead tables.
+Status graph_finish(DeviceGraph &gr, const int32_t *deg, int32_t *d_old_off, int32_t *d_old_adj)
+{
+    DeviceGraph *g = &gr;
+    const int32_t V = g->V;
+    const int64_t nnz = g->nnz;
     int32_t maxd = 0;
-    for (int32_t v = 0; v < V; ++v) { deg[v] = offsets[v + 1] - offsets[v]; maxd = std::max(maxd, deg[v]); }
+    for (int32_t v = 0; v < V; ++v) maxd = std::max(maxd, deg[v]);
     g->max_degree = maxd;
     std::vector<int64_t> bucket((size_t)maxd + 2, 0);
     for (int32_t v = 0; v < V; ++v) bucket[(size_t)(maxd - deg[v]) + 1]++;
@@ -454,29 +459,16 @@ Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V,
         g->h_degree[i] = deg[iperm[i]];
         noff[i + 1] = noff[i] + g->h_degree[i];
     }
-    SG_CK(cudaMallocAsync(&g->d_off, sizeof(int32_t) * ((size_t)V + 1), g->stream));
-    SG_CK(cudaMallocAsync(&g->d_adj, sizeof(int32_t) * std::max<int64_t>(nnz, 1), g->stream));
-    SG_CK(cudaMallocAsync(&g->d_perm, sizeof(int32_t) * std::max<int32_t>(V, 1), g->stream));
-    SG_CK(cudaMallocAsync(&g->d_iperm, sizeof(int32_t) * std::max<int32_t>(V, 1), g->stream));
-    int32_t *d_old_off = nullptr, *d_old_adj = nullptr;
-    SG_CK(cudaMallocAsync(&d_old_off, sizeof(int32_t) * ((size_t)V + 1), g->stream));
-    SG_CK(cudaMallocAsync(&d_old_adj, sizeof(int32_t) * std::max<int64_t>(nnz, 1), g->stream));
     cudaStream_t st = g->stream;
-    SG_CK(cudaMemcpyAsync(d_old_off, offsets, sizeof(int32_t) * ((size_t)V + 1), cudaMemcpyHostToDevice, st));
-    if (nnz) SG_CK(cudaMemcpyAsync(d_old_adj, neighbors, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
+    SG_CK(cudaMallocAsync(&g->d_off, sizeof(int32_t) * ((size_t)V + 1), st));
+    SG_CK(cudaMallocAsync(&g->d_adj, sizeof(int32_t) * std::max<int64_t>(nnz, 1), st));
+    SG_CK(cudaMallocAsync(&g->d_perm, sizeof(int32_t) * std::max<int32_t>(V, 1), st));
+    SG_CK(cudaMallocAsync(&g->d_iperm, sizeof(int32_t) * std::max<int32_t>(V, 1), st));
     SG_CK(cudaMemcpyAsync(g->d_off, noff.data(), sizeof(int32_t) * ((size_t)V + 1), cudaMemcpyHostToDevice, st));
     if (V) {
         SG_CK(cudaMemcpyAsync(g->d_perm, perm.data(), sizeof(int32_t) * V, cudaMemcpyHostToDevice, st));
         SG_CK(cudaMemcpyAsync(g->d_iperm, iperm.data(), sizeof(int32_t) * V, cudaMemcpyHostToDevice, st));
     }
-    // neighbour ids are range-checked on the host before the remap reads them
-    for (int64_t e = 0; e < nnz; ++e)
-        if ((uint32_t)neighbors[e] >= (uint32_t)V) {
-            cudaFreeAsync(d_old_off, st);
-            cudaFreeAsync(d_old_adj, st);
-            cudaStreamSynchronize(st);
-            return Status{1, "neighbour id out of range at entry " + std::to_string(e)};
-        }
     launch_remap(V, d_old_off, d_old_adj, g->d_off, g->d_iperm, g->d_perm, g->d_adj, st);
     SG_CK(cudaGetLastError());
     // coloring jump-ahead tables
@@ -496,13 +488,38 @@ Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V,
         q[0] = top;
         q[28] += top;
     }
-    SG_CK(cudaMallocAsync(&g->d_jump, jump.size() * 4, g->stream));
-    SG_CK(cudaMallocAsync(&g->d_coef, coef.size() * 4, g->stream));
+    SG_CK(cudaMallocAsync(&g->d_jump, jump.size() * 4, st));
+    SG_CK(cudaMallocAsync(&g->d_coef, coef.size() * 4, st));
     SG_CK(cudaMemcpyAsync(g->d_jump, jump.data(), jump.size() * 4, cudaMemcpyHostToDevice, st));
     SG_CK(cudaMemcpyAsync(g->d_coef, coef.data(), coef.size() * 4, cudaMemcpyHostToDevice, st));
     cudaFreeAsync(d_old_off, st);
     cudaFreeAsync(d_old_adj, st);
     SG_CK(cudaStreamSynchronize(st));
+    return Status::ok();
+}
+
+Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V, int64_t nnz, int device,
+                    std::unique_ptr<DeviceGraph> &out)
+{
+    if (V < 0 || nnz < 0 || nnz > 0x7fffffffLL) return Status{1, "vertex or entry count out of range"};
+    if (!offsets || (nnz > 0 && !neighbors)) return Status{1, "null graph array"};
+    if (offsets[0] != 0 || offsets[V] != nnz) return Status{1, "offsets[0] must be 0 and offsets[V] must equal nnz"};
+    for (int32_t v = 0; v < V; ++v)
+        if (offsets[v + 1] < offsets[v]) return Status{1, "offsets are not monotone"};
+    // neighbour ids are range-checked on the host before the remap reads them
+    for (int64_t e = 0; e < nnz; ++e)
+        if ((uint32_t)neighbors[e] >= (uint32_t)V) return Status{1, "neighbour id out of range at entry " + std::to_string(e)};
+    std::unique_ptr<DeviceGraph> g;
+    SG_CKS(new_device_graph(device, V, nnz, g));
+    std::vector<int32_t> deg(V);
+    for (int32_t v = 0; v < V; ++v) deg[v] = offsets[v + 1] - offsets[v];
+    int32_t *d_old_off = nullptr, *d_old_adj = nullptr;
+    cudaStream_t st = g->stream;
+    SG_CK(cudaMallocAsync(&d_old_off, sizeof(int32_t) * ((size_t)V + 1), st));
+    SG_CK(cudaMallocAsync(&d_old_adj, sizeof(int32_t) * std::max<int64_t>(nnz, 1), st));
+    SG_CK(cudaMemcpyAsync(d_old_off, offsets, sizeof(int32_t) * ((size_t)V + 1), cudaMemcpyHostToDevice, st));
+    if (nnz) SG_CK(cudaMemcpyAsync(d_old_adj, neighbors, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
+    SG_CKS(graph_finish(*g, deg.data(), d_old_off, d_old_adj));
     out = std::move(g);
     return Status::ok();
 }

@@ -76,6 +76,28 @@ struct CountStats {
 Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V, int64_t nnz, int device,
                     std::unique_ptr<DeviceGraph> &out);
 
+// Pieces of a graph upload shared by the host-array and device-array paths:
+// a DeviceGraph with its stream, and the tail that orders the vertices by
+// degree (from the V host degrees), relabels the original-order device
+// adjacency (freed here) and builds the coloring tables.
+Status new_device_graph(int device, int32_t V, int64_t nnz, std::unique_ptr<DeviceGraph> &out);
+Status graph_finish(DeviceGraph &g, const int32_t *deg, int32_t *d_old_off, int32_t *d_old_adj);
+
+// Input preparation on the GPU (engine/input_gpu.cu), each ending in a
+// DeviceGraph without a host copy of the adjacency:
+//   graph_from_edges   host edge arrays -> CSC of the symmetrised adjacency
+//                      (CSCGraph::createFromEdgeListFile semantics) on the GPU
+//   graph_from_text    an edge-list text file ("V\nE\nu v\n...", EdgeList.cpp:34-116)
+//                      parsed on the GPU, hole removal included
+//   graph_from_rmat    an R-MAT graph generated, deduplicated and built on the GPU
+// and graph_download_csc: the CSC in original vertex order back to the host.
+Status graph_from_edges(int32_t V, const int32_t *src, const int32_t *dst, int64_t E, int device,
+                        std::unique_ptr<DeviceGraph> &out);
+Status graph_from_text(const std::string &path, int device, std::unique_ptr<DeviceGraph> &out);
+Status graph_from_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed, int device,
+                       std::unique_ptr<DeviceGraph> &out);
+Status graph_download_csc(DeviceGraph &g, int32_t *offsets, int32_t *neighbors);
+
 // Runs n_colorings colorings, writes the raw colorful counts (host).
 Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, CountStats *stats);
 
