@@ -147,6 +147,15 @@ struct LineStart {
     __host__ __device__ bool operator()(int64_t i) const { return i == 0 || text[i - 1] == '\n'; }
 };
 
+__global__ void k_count_lines(const char *__restrict__ text, int64_t n, unsigned long long *count)
+{
+    unsigned long long c = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        c += (i == 0 || text[i - 1] == '\n') ? 1 : 0;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+
 __global__ void k_parse_lines(const char *__restrict__ text, int64_t n, const int64_t *__restrict__ starts,
                               int64_t nlines, int64_t E, int32_t *__restrict__ src, int32_t *__restrict__ dst,
                               int32_t *err, int32_t *max_id)
@@ -328,15 +337,21 @@ Status graph_from_text(const std::string &path, int device, std::unique_ptr<Devi
     int64_t *d_starts = nullptr, *d_nlines = nullptr;
     int32_t *d_src = nullptr, *d_dst = nullptr, *d_err = nullptr, *d_max = nullptr;
     IG_CK(cudaMallocAsync(&d_text, (size_t)std::max<int64_t>(n, 1), st));
-    IG_CK(cudaMallocAsync(&d_starts, 8 * (size_t)std::max<int64_t>(n, 1), st));
     IG_CK(cudaMallocAsync(&d_nlines, 8, st));
+    IG_CK(cudaMemsetAsync(d_nlines, 0, 8, st));
+    if (n) IG_CK(cudaMemcpyAsync(d_text, p, (size_t)n, cudaMemcpyHostToDevice, st));
+    // count the line starts first: the selection output holds exactly them
+    unsigned long long nstart = 0;
+    if (n) k_count_lines<<<grid_for(n), 256, 0, st>>>(d_text, n, reinterpret_cast<unsigned long long *>(d_nlines));
+    IG_CK(cudaMemcpyAsync(&nstart, d_nlines, 8, cudaMemcpyDeviceToHost, st));
+    IG_CK(cudaStreamSynchronize(st));
+    IG_CK(cudaMallocAsync(&d_starts, 8 * (size_t)std::max<unsigned long long>(nstart, 1), st));
     IG_CK(cudaMallocAsync(&d_src, 4 * (size_t)std::max(E, 1), st));
     IG_CK(cudaMallocAsync(&d_dst, 4 * (size_t)std::max(E, 1), st));
     IG_CK(cudaMallocAsync(&d_err, 8, st));
     d_max = d_err + 1;
     IG_CK(cudaMemsetAsync(d_err, 0, 8, st));
     IG_CK(cudaMemsetAsync(d_nlines, 0, 8, st));
-    if (n) IG_CK(cudaMemcpyAsync(d_text, p, (size_t)n, cudaMemcpyHostToDevice, st));
     // line starts: positions i with i == 0 or text[i-1] == '\n'
     size_t tmp_bytes = 0;
     void *tmp = nullptr;
