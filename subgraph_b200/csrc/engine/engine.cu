@@ -101,6 +101,8 @@ struct Workspace {
     size_t chunk_start_bytes = 0;
     double *root_vertex = nullptr;
     size_t root_vertex_bytes = 0;
+    int32_t *adjc = nullptr;           // [nnz] neighbour id | color << 28 of the coloring in slot 0
+    size_t adjc_bytes = 0;
     uint64_t generation = 0;   // bumped whenever a buffer above is re-allocated
 };
 
@@ -110,6 +112,9 @@ struct DevicePlanTables {
     std::vector<uint32_t *> aoff, moff;  // per sub: packed-layout byte offsets (FP32)
     std::vector<int32_t *> blk;      // per sub: register-blocked eMA column tables, or null
     std::vector<int32_t> blk_shape, blk_nblocks;
+    // per sub with a non-leaf aux child: [k][chunks] masks for chunks of 4 / 2 columns
+    std::vector<uint16_t *> cmask4, cmask2;
+    std::vector<int32_t> cm4_stride, cm2_stride;
 };
 
 // The work queue of one batch shape (plan, slots, mode, hubs), built once per
@@ -299,8 +304,58 @@ bool build_blocks(const Plan &p, int s, std::vector<int32_t> &rows, int &nblocks
     return true;
 }
 
+// the `size` colors (ascending) of the color set with colex rank r
+void colex_unrank(int size, int64_t r, int *out)
+{
+    for (int t = size; t >= 1; --t) {
+        int x = t - 1;
+        while (binom(x + 1, t) <= r) ++x;
+        out[t - 1] = x;
+        r -= binom(x, t);
+    }
+}
+
+// Chunk masks of sub s's aggregation (aux child of >= 2 colors): bit c_u of
+// mask[c][j] is set when column chunk j (w columns) holds a color set that
+// contains c_u and lacks c.  A vertex of color c reads chunk j of a
+// neighbour of color c_u only then: the neighbour's other entries are exact
+// zeros (its own color is in every non-zero set), and the columns containing
+// c are read by no output or meet a main entry that is an exact zero.
+Status upload_chunk_masks(DeviceGraph &g, const Plan &p, int s, DevicePlanTables &out)
+{
+    const SubTemplate &a = p.subs[p.subs[s].aux];
+    const int k = p.k, na = a.size;
+    if (na < 2 || k > 16) return Status::ok();
+    std::vector<unsigned> am(a.L);
+    int el[32];
+    for (int t = 0; t < a.L; ++t) {
+        colex_unrank(na, t, el);
+        unsigned m = 0;
+        for (int i = 0; i < na; ++i) m |= 1u << el[i];
+        am[t] = m;
+    }
+    for (int w : {4, 2}) {
+        const int nch = (a.L + w - 1) / w;
+        std::vector<uint16_t> cm((size_t)k * nch, 0);
+        for (int c = 0; c < k; ++c)
+            for (int j = 0; j < nch; ++j)
+                for (int t = j * w; t < std::min(a.L, j * w + w); ++t)
+                    if (!(am[t] >> c & 1)) cm[(size_t)c * nch + j] |= (uint16_t)(am[t] & 0xffffu);
+        uint16_t *&dst = w == 4 ? out.cmask4[s] : out.cmask2[s];
+        SG_CK(cudaMallocAsync(&dst, cm.size() * 2, g.stream));
+        SG_CK(cudaMemcpyAsync(dst, cm.data(), cm.size() * 2, cudaMemcpyHostToDevice, g.stream));
+        SG_CK(cudaStreamSynchronize(g.stream));   // `cm` is pageable and goes out of scope
+        (w == 4 ? out.cm4_stride : out.cm2_stride)[s] = nch;
+    }
+    return Status::ok();
+}
+
 Status upload_plan(DeviceGraph &g, const Plan &p, DevicePlanTables &out)
 {
+    out.cmask4.assign(p.nsub(), nullptr);
+    out.cmask2.assign(p.nsub(), nullptr);
+    out.cm4_stride.assign(p.nsub(), 0);
+    out.cm2_stride.assign(p.nsub(), 0);
     out.blk.assign(p.nsub(), nullptr);
     out.blk_shape.assign(p.nsub(), 0);
     out.blk_nblocks.assign(p.nsub(), 0);
@@ -359,6 +414,7 @@ Status upload_plan(DeviceGraph &g, const Plan &p, DevicePlanTables &out)
             SG_CK(cudaMallocAsync(&out.rem[s], rem.size() * 2, g.stream));
             SG_CK(cudaMemcpyAsync(out.rem[s], rem.data(), rem.size() * 2, cudaMemcpyHostToDevice, g.stream));
         }
+        SG_CKS(upload_chunk_masks(g, p, s, out));
     }
     SG_CK(cudaStreamSynchronize(g.stream));
     return Status::ok();
@@ -396,7 +452,7 @@ DeviceGraph::~DeviceGraph()
         if (it != g_state.end()) {
             Workspace &w = it->second.ws;
             for (void *p : {w.arena, (void *)w.colors, (void *)w.partial, (void *)w.raw, (void *)w.windows, w.hub_partial,
-                            (void *)w.chunk_start, (void *)w.root_vertex})
+                            (void *)w.chunk_start, (void *)w.root_vertex, (void *)w.adjc})
                 if (p) cudaFreeAsync(p, stream);
             for (auto &kv : it->second.plans) {
                 for (auto *p : kv.second.split) if (p) cudaFreeAsync(p, stream);
@@ -404,6 +460,8 @@ DeviceGraph::~DeviceGraph()
                 for (auto *p : kv.second.aoff) if (p) cudaFreeAsync(p, stream);
                 for (auto *p : kv.second.blk) if (p) cudaFreeAsync(p, stream);
                 for (auto *p : kv.second.moff) if (p) cudaFreeAsync(p, stream);
+                for (auto *p : kv.second.cmask4) if (p) cudaFreeAsync(p, stream);
+                for (auto *p : kv.second.cmask2) if (p) cudaFreeAsync(p, stream);
             }
             for (auto &kv : it->second.batches) free_batch(kv.second, stream);
             g_state.erase(it);
@@ -546,6 +604,7 @@ struct RunCtx {
     int lay = 1;             // colorings interleaved per table row (grouped batched form)
     size_t arena_base = 0;   // byte offset of this context's tables in the arena (job queues)
     bool exact = false;      // no fused products (packed eMA), no hub chunks
+    bool use_adjc = false;   // one coloring at a time in slot 0: neighbour ids carry their colors
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> fused_ev, hub_ev;
     std::vector<std::pair<int, double>> fused_sub;   // per fused launch: sub, compulsory bytes
     double fused_alg_bytes = 0, fused_gather_bytes = 0;
@@ -611,6 +670,7 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
     SG_CKS(growT(&w.partial, &w.partial_bytes, 8 * ((V / 8 + 2) * ncolor_slots), g.stream));
     SG_CKS(growT(&w.raw, &w.raw_bytes, 8 * (size_t)std::max(ncolorings_total, 1), g.stream));
     SG_CKS(growT(&w.windows, &w.windows_bytes, 4 * 31 * (size_t)std::max(ncolorings_total, 1), g.stream));
+    if (c.use_adjc) SG_CKS(growT(&w.adjc, &w.adjc_bytes, std::max<size_t>(16, 4 * (size_t)g.nnz), g.stream));
     if (c.hubs.count > 0) {
         // a partial row holds the aux columns (or colour counts) of up to c.lay colorings
         int32_t maxp = round_up(c.lay * c.p.k, 4);
@@ -636,6 +696,9 @@ void *table_ptr(RunCtx &c, int slot, int sub)
     return (char *)c.gs.ws.arena + c.arena_base + c.arena_per_coloring * slot +
            (size_t)c.lay * c.p.table_offset[sub] * c.g.V * c.es;
 }
+
+// neighbour ids with their color in the top 4 bits: ids below 2^28, colors below 16
+bool adjc_ok(const DeviceGraph &g, const Plan &p) { return g.V < (1 << 28) && p.k <= 16 && g.nnz > 0; }
 
 // The descriptor of one sub-template step of the coloring in color slot `slot`,
 // or of colorings [b0, b0 + nb) of an interleaved group (c.lay > 1, slot 0);
@@ -689,6 +752,11 @@ StageDesc make_stage(RunCtx &c, int slot, int s, double *root_vertex, int b0 = 0
     d.blk_shape = d.blk ? c.tab->blk_shape[s] : 0;
     d.blk_nblocks = d.blk ? c.tab->blk_nblocks[s] : 0;
     d.color = w.colors + (size_t)slot * g.V + b0;
+    if (c.use_adjc && slot == 0 && L == 1) {
+        d.adjc = w.adjc;
+        d.cmask = c.fp64 ? c.tab->cmask2[s] : c.tab->cmask4[s];
+        d.cmask_stride = c.fp64 ? c.tab->cm2_stride[s] : c.tab->cm4_stride[s];
+    }
     d.off = g.d_off;
     d.adj = g.d_adj;
     d.root_partial = w.partial + (size_t)(slot + b0) * (g.V / 8 + 2);
@@ -816,6 +884,8 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
     return Status::ok();
 }
 
+// Colors of colorings [first_coloring, +n) into slots [slot0, +n); on the
+// one-coloring-at-a-time path also the colored adjacency of slot 0.
 Status launch_colors(RunCtx &c, int slot0, int first_coloring, int n, cudaStream_t st)
 {
     ColorArgs a{};
@@ -831,6 +901,10 @@ Status launch_colors(RunCtx &c, int slot0, int first_coloring, int n, cudaStream
     a.vertex_stride = c.lay;
     launch_color(a, n, st);
     c.launches += 1;
+    if (c.use_adjc && c.lay == 1 && slot0 == 0 && n == 1) {
+        launch_color_adj(c.g.d_adj, c.g.nnz, c.gs.ws.colors, c.gs.ws.adjc, st);
+        c.launches += 1;
+    }
     SG_CK(cudaGetLastError());
     return Status::ok();
 }
@@ -1306,6 +1380,7 @@ Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, 
     if (o.n_colorings < 1) return Status{1, "n_colorings must be >= 1"};
     if (o.mode < 0 || o.mode > 2) return Status{1, "unknown count mode"};
     if (p.k > 255) return Status{1, "too many colors"};
+    if (g.V >= (1 << 28)) return Status{1, "counting supports graphs of fewer than 2^28 vertices"};
     SG_CK(cudaSetDevice(g.device));
     GraphState &gs = state_of(g);
     RunCtx c{g, p, gs, nullptr, o.mode == kModeFP64, (size_t)(o.mode == kModeFP64 ? 8 : 4), 0, {}, 0, 0, o.mode, 0};
@@ -1317,6 +1392,7 @@ Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, 
     c.blocked = o.blocked != 0;
     if (o.batch > 0) return o.persistent ? count_batched(c, o, raw, stats) : count_grouped(c, o, raw, stats);
     const int slots = 1;
+    c.use_adjc = adjc_ok(g, p);
     SG_CKS(prepare(c, slots, o.n_colorings));
     SG_CKS(upload_windows(c, o.seed_base, o.n_colorings));
     cudaStream_t st = g.stream;
@@ -1381,10 +1457,12 @@ Status debug_colors(DeviceGraph &g, int k, uint32_t seed, int32_t *colors)
 static Status run_partial(DeviceGraph &g, const Plan &p, uint32_t seed, int mode, int hub_threshold, int upto,
                           RunCtx &c, GraphState &gs)
 {
+    if (g.V >= (1 << 28)) return Status{1, "counting supports graphs of fewer than 2^28 vertices"};
     SG_CKS(make_ctx_tables(g, p, gs, c.tab));
     // the parity helpers are exact when no hub chunking is asked for
     c.exact = hub_threshold == 0;
     c.hubs = plan_hubs(g, hub_threshold);
+    c.use_adjc = adjc_ok(g, p);
     SG_CKS(prepare(c, 1, 1));
     SG_CKS(upload_windows(c, seed, 1));
     SG_CKS(launch_colors(c, 0, 0, 1, g.stream));
@@ -1473,6 +1551,7 @@ Status count_jobs(DeviceGraph &g, const std::vector<const Plan *> &plans, const 
     if (o.mode < 0 || o.mode > 2) return Status{1, "unknown count mode"};
     for (const Plan *p : plans)
         if (!p) return Status{1, "null template plan"};
+    if (g.V >= (1 << 28)) return Status{1, "counting supports graphs of fewer than 2^28 vertices"};
     SG_CK(cudaSetDevice(g.device));
     GraphState &gs = state_of(g);
     Workspace &w = gs.ws;

@@ -112,11 +112,26 @@ __global__ void __launch_bounds__(NT) k_hub(HubArgs h)
     for (int item = blockIdx.x; item < h.total_chunks; item += gridDim.x) hub_item<T, NT>(h, item, smem_raw);
 }
 
-void choose_gather(StageDesc &d, bool fp64)
+// Threads per vertex (gather_group) and chunks per thread (gather_q) of the
+// aggregation: Q = `want`, or the smallest Q that keeps nine in ten threads
+// busy.  False when Q = `want` needs more threads than the CTA has.
+bool choose_gather(StageDesc &d, bool fp64, int want = 0)
 {
+    if (d.aux_leaf) {
+        d.gather_q = 1;
+        d.gather_group = 1;
+        return want <= 1;
+    }
     const int CH = fp64 ? 2 : 4;
     const int nchunk = (d.aux_cols + CH - 1) / CH;
     const int NT = d.nthreads;
+    if (want > 0) {
+        const int G = (nchunk + want - 1) / want;
+        if (G > NT) return false;
+        d.gather_q = want;
+        d.gather_group = std::max(1, G);
+        return true;
+    }
     int bestQ = 4, bestG = (nchunk + 3) / 4, bestActive = -1;
     for (int Q : {1, 2, 4}) {
         const int G = (nchunk + Q - 1) / Q;
@@ -125,8 +140,9 @@ void choose_gather(StageDesc &d, bool fp64)
         if (active >= (NT * 9) / 10) { bestQ = Q; bestG = G; bestActive = active; break; }
         if (active > bestActive) { bestQ = Q; bestG = G; bestActive = active; }
     }
-    d.gather_q = d.aux_leaf ? 1 : bestQ;
-    d.gather_group = d.aux_leaf ? 1 : std::max(1, bestG);
+    d.gather_q = bestQ;
+    d.gather_group = std::max(1, bestG);
+    return true;
 }
 
 bool packed_ok(const StageDesc &d, bool fp64, int tv)
@@ -172,8 +188,7 @@ bool set_shape(StageDesc &d, bool fp64, const TileShape &sh)
     d.out_chunk = oc;
     d.smem = bytes;
     d.ntiles = (d.V + sh.tile_v - 1) / sh.tile_v;
-    choose_gather(d, fp64);
-    return true;
+    return choose_gather(d, fp64, sh.q);
 }
 
 std::vector<TileShape> candidate_shapes(const StageDesc &d, bool fp64)
@@ -193,7 +208,21 @@ std::vector<TileShape> candidate_shapes(const StageDesc &d, bool fp64)
     for (auto &c : all) {
         size_t bytes;
         int oc;
-        if (shape_fits(d, fp64, c.tile_v, c.threads, c.packed, 227 * 1024, bytes, oc)) out.push_back(c);
+        if (!shape_fits(d, fp64, c.tile_v, c.threads, c.packed, 227 * 1024, bytes, oc)) continue;
+        out.push_back(c);
+        // wide aggregations: also the other chunk counts per thread (more chunks
+        // per thread share one neighbour id and row address among them)
+        if (!d.aux_leaf && d.aux_cols >= 64) {
+            StageDesc e = d;
+            if (!set_shape(e, fp64, c)) continue;
+            for (int q : {1, 2, 4}) {
+                if (q == e.gather_q) continue;
+                TileShape t = c;
+                t.q = q;
+                StageDesc f = d;
+                if (set_shape(f, fp64, t)) out.push_back(t);
+            }
+        }
     }
     return out;
 }
@@ -283,6 +312,24 @@ void launch_hub(const HubArgs &h, bool fp64, int sm_count, cudaStream_t st)
     const int grid = std::max(1, std::min(h.total_chunks, sm_count * 8));
     if (fp64) k_hub<double, 256><<<grid, 256, 0, st>>>(h);
     else k_hub<float, 256><<<grid, 256, 0, st>>>(h);
+}
+
+// ---------------------------------------------------------------------------
+// Colored adjacency of one coloring: neighbour id | its color << 28.
+__global__ void k_color_adj(const int32_t *__restrict__ adj, int64_t nnz, const uint8_t *__restrict__ color,
+                            int32_t *__restrict__ adjc)
+{
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t u = adj[e];
+        adjc[e] = u | ((int32_t)color[u] << 28);
+    }
+}
+
+void launch_color_adj(const int32_t *adj, int64_t nnz, const uint8_t *color, int32_t *adjc, cudaStream_t st)
+{
+    if (nnz <= 0) return;
+    const int grid = (int)std::min<int64_t>((nnz + 255) / 256, 148 * 32);
+    k_color_adj<<<grid, 256, 0, st>>>(adj, nnz, color, adjc);
 }
 
 // ---------------------------------------------------------------------------

@@ -32,6 +32,8 @@ struct ColorArgs {
 };
 
 void launch_color(const ColorArgs &a, int ncolorings, cudaStream_t st);
+// adjc[e] = adj[e] | color[adj[e]] << 28 (ids below 2^28, colors below 16)
+void launch_color_adj(const int32_t *adj, int64_t nnz, const uint8_t *color, int32_t *adjc, cudaStream_t st);
 void launch_remap(int32_t V, const int32_t *old_off, const int32_t *old_adj, const int32_t *new_off,
                   const int32_t *iperm, const int32_t *perm, int32_t *new_adj, cudaStream_t st);
 
@@ -50,6 +52,8 @@ struct TileShape {
     int tile_v;      // vertices per tile
     int threads;     // CTA size
     int packed;      // eMA form: 0 per-output loop, 1 packed FP32x2 (32-vertex tiles), 2 register-blocked
+    int q = 0;       // 16-byte column chunks per aggregation thread (1, 2, 4); 0: the fewest that keep
+                     // nine in ten threads busy
 };
 // Sets an explicit shape (the autotuner's candidates); false when it does not fit.
 bool set_shape(StageDesc &d, bool fp64, const TileShape &shape);

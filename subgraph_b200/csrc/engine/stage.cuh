@@ -62,6 +62,15 @@ struct StageDesc {
     int32_t blk_shape;                 // blk::shape_id of (|s|, |main|), 0 = no blocked form
     int32_t blk_nblocks;
     const int16_t *rem;                // [L_s][k] main-leaf: aux column of set\{c}, or -1
+    // One coloring at a time: adjc[e] = neighbour id | its color << 28.  A
+    // vertex of color c only reads aggregate columns without c (the others
+    // meet a main entry that is an exact zero, or no output at all), and a
+    // neighbour of color c_u only adds to sets containing c_u (its other
+    // entries are exact zeros): cmask[c][chunk] has bit c_u set when the
+    // 16-byte column chunk holds such a set; other chunks are skipped.
+    const int32_t *adjc;               // [nnz], or null (adj)
+    const uint16_t *cmask;             // [k][cmask_stride] (with adjc, non-leaf aux), or null: every chunk read
+    int32_t cmask_stride;
     const uint8_t *color;              // [V] internal order
     const int32_t *off;                // [V+1]
     const int32_t *adj;                // [nnz]

@@ -215,26 +215,88 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
 #pragma unroll
                     for (int r = 0; r < Q; ++r) acc[r] = CT::zero();
                     const int beg = __ldg(d.off + v), end = __ldg(d.off + v + 1);
-                    // batches of U neighbours with all their row loads in flight;
-                    // the last batch is predicated and its idle slots add +0,
-                    // which leaves every (non-negative) sum bit-identical
-                    for (int e = beg; e < end; e += U) {
-                        int nb[U];
+                    const int32_t *nbrs = d.adjc ? d.adjc : d.adj;
+                    if (d.cmask) {
+                        // colored neighbour ids: chunk q of a neighbour of color c_u is
+                        // read only when bit c_u of this vertex color's mask is set
+                        // (other chunks: exact zeros, or columns whose products meet
+                        // an exact zero); a skipped slot adds +0
+                        const uint16_t *cm = d.cmask + (size_t)__ldg(d.color + v) * d.cmask_stride;
+                        uint32_t msk[Q];
 #pragma unroll
-                        for (int u = 0; u < U; ++u) nb[u] = e + u < end ? __ldg(d.adj + e + u) : -1;
-                        C x[U][Q];
+                        for (int r = 0; r < Q; ++r) {
+                            const int q = lane_g + G * r;
+                            msk[r] = q < nchunk ? (uint32_t)__ldg(cm + q) : 0u;
+                        }
+                        for (int e = beg; e < end; e += U) {
+                            int nw[U];
 #pragma unroll
-                        for (int u = 0; u < U; ++u)
+                            for (int u = 0; u < U; ++u) nw[u] = e + u < end ? __ldg(nbrs + e + u) : 0;
+                            C x[U][Q];
 #pragma unroll
-                            for (int r = 0; r < Q; ++r) {
-                                const int q = lane_g + G * r;
-                                x[u][r] = (q < nchunk && nb[u] >= 0) ? ld_tab<COH>(auxc + (size_t)nb[u] * rowc + q)
-                                                                     : CT::zero();
+                            for (int u = 0; u < U; ++u)
+#pragma unroll
+                                for (int r = 0; r < Q; ++r) {
+                                    const int q = lane_g + G * r;
+                                    x[u][r] = (e + u < end && ((msk[r] >> ((uint32_t)nw[u] >> 28)) & 1u))
+                                                  ? ld_tab<COH>(auxc + (size_t)(nw[u] & 0x0fffffff) * rowc + q)
+                                                  : CT::zero();
+                                }
+#pragma unroll
+                            for (int u = 0; u < U; ++u)
+#pragma unroll
+                                for (int r = 0; r < Q; ++r) CT::add(acc[r], x[u][r]);
+                        }
+                    } else if (lane_g + G * (Q - 1) < nchunk) {
+                        // every slot of this thread lies in the row: full batches of U
+                        // neighbours without predicates, then the remaining ones singly
+                        // (the same neighbour order, so the same sums)
+                        const C *base = auxc + lane_g;
+                        int e = beg;
+                        for (; e + U <= end; e += U) {
+                            int nb[U];
+#pragma unroll
+                            for (int u = 0; u < U; ++u) nb[u] = __ldg(nbrs + e + u) & 0x0fffffff;
+                            C x[U][Q];
+#pragma unroll
+                            for (int u = 0; u < U; ++u) {
+                                const C *row = base + (size_t)nb[u] * rowc;
+#pragma unroll
+                                for (int r = 0; r < Q; ++r) x[u][r] = ld_tab<COH>(row + G * r);
                             }
 #pragma unroll
-                        for (int u = 0; u < U; ++u)
+                            for (int u = 0; u < U; ++u)
 #pragma unroll
-                            for (int r = 0; r < Q; ++r) CT::add(acc[r], x[u][r]);
+                                for (int r = 0; r < Q; ++r) CT::add(acc[r], x[u][r]);
+                        }
+                        for (; e < end; ++e) {
+                            const C *row = base + (size_t)(__ldg(nbrs + e) & 0x0fffffff) * rowc;
+                            C x[Q];
+#pragma unroll
+                            for (int r = 0; r < Q; ++r) x[r] = ld_tab<COH>(row + G * r);
+#pragma unroll
+                            for (int r = 0; r < Q; ++r) CT::add(acc[r], x[r]);
+                        }
+                    } else {
+                        // some slots past the row (the last threads of the group)
+                        for (int e = beg; e < end; e += U) {
+                            int nb[U];
+#pragma unroll
+                            for (int u = 0; u < U; ++u) nb[u] = e + u < end ? (__ldg(nbrs + e + u) & 0x0fffffff) : -1;
+                            C x[U][Q];
+#pragma unroll
+                            for (int u = 0; u < U; ++u)
+#pragma unroll
+                                for (int r = 0; r < Q; ++r) {
+                                    const int q = lane_g + G * r;
+                                    x[u][r] = (q < nchunk && nb[u] >= 0) ? ld_tab<COH>(auxc + (size_t)nb[u] * rowc + q)
+                                                                         : CT::zero();
+                                }
+#pragma unroll
+                            for (int u = 0; u < U; ++u)
+#pragma unroll
+                                for (int r = 0; r < Q; ++r) CT::add(acc[r], x[u][r]);
+                        }
                     }
                 }
 #pragma unroll
