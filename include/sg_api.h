@@ -178,7 +178,9 @@ typedef struct {
 void sg_count_opts_default(sg_count_opts *o);
 
 /* CountMat::colorCounting per coloring (CountMat.cpp:268-322): raw colorful
- * counts, one per coloring, into raw[n_colorings] (host). */
+ * counts, one per coloring, into raw[n_colorings] (host).  Graphs of 2^28 or
+ * more vertices are rejected (SG_ERR_INVALID): neighbour ids carry their
+ * color in the top 4 bits of a 32-bit word. */
 sg_status sg_count(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw, sg_count_stats *stats);
 
 /* A stream of jobs with different templates on one graph: job j counts one
