@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
     k_persistent(const BatchStage *__restrict__ stages, int nstages, int total_items, int *done, BatchCtl *ctl,
                  long long wait_cycles, unsigned long long *stage_end)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(32) unsigned char smem_raw[];
     __shared__ BatchStage st;
     __shared__ int s_item, s_stage, s_skip, s_cur;
     if (threadIdx.x == 0) s_cur = -1;   // the stage whose descriptor is in `st`

@@ -21,7 +21,7 @@ template <int NT, int Q, int N, int P>
 __global__ void __launch_bounds__(NT, (NT == 512 ? blk_min_blocks<N, P>() : 2 * blk_min_blocks<N, P>()))
     k_fused_blk(StageDesc d)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(32) unsigned char smem_raw[];
     for (int tile = blockIdx.x; tile < d.ntiles; tile += gridDim.x)
         fused_tile<float, NT, Q, false, false, true, N, P>(d, tile, smem_raw);
 }

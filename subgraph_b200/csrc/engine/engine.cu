@@ -112,9 +112,9 @@ struct DevicePlanTables {
     std::vector<uint32_t *> aoff, moff;  // per sub: packed-layout byte offsets (FP32)
     std::vector<int32_t *> blk;      // per sub: register-blocked eMA column tables, or null
     std::vector<int32_t> blk_shape, blk_nblocks;
-    // per sub with a non-leaf aux child: [k][chunks] masks for chunks of 4 / 2 columns
-    std::vector<uint16_t *> cmask4, cmask2;
-    std::vector<int32_t> cm4_stride, cm2_stride;
+    // per sub with a non-leaf aux child: [k][chunks] masks for 32-byte chunks (8 FP32 / 4 FP64 columns)
+    std::vector<uint16_t *> cmask_f32, cmask_f64;
+    std::vector<int32_t> cmf32_stride, cmf64_stride;
 };
 
 // The work queue of one batch shape (plan, slots, mode, hubs), built once per
@@ -334,28 +334,28 @@ Status upload_chunk_masks(DeviceGraph &g, const Plan &p, int s, DevicePlanTables
         for (int i = 0; i < na; ++i) m |= 1u << el[i];
         am[t] = m;
     }
-    for (int w : {4, 2}) {
+    for (int w : {8, 4}) {   // chunk columns: FP32, FP64
         const int nch = (a.L + w - 1) / w;
         std::vector<uint16_t> cm((size_t)k * nch, 0);
         for (int c = 0; c < k; ++c)
             for (int j = 0; j < nch; ++j)
                 for (int t = j * w; t < std::min(a.L, j * w + w); ++t)
                     if (!(am[t] >> c & 1)) cm[(size_t)c * nch + j] |= (uint16_t)(am[t] & 0xffffu);
-        uint16_t *&dst = w == 4 ? out.cmask4[s] : out.cmask2[s];
+        uint16_t *&dst = w == 8 ? out.cmask_f32[s] : out.cmask_f64[s];
         SG_CK(cudaMallocAsync(&dst, cm.size() * 2, g.stream));
         SG_CK(cudaMemcpyAsync(dst, cm.data(), cm.size() * 2, cudaMemcpyHostToDevice, g.stream));
         SG_CK(cudaStreamSynchronize(g.stream));   // `cm` is pageable and goes out of scope
-        (w == 4 ? out.cm4_stride : out.cm2_stride)[s] = nch;
+        (w == 8 ? out.cmf32_stride : out.cmf64_stride)[s] = nch;
     }
     return Status::ok();
 }
 
 Status upload_plan(DeviceGraph &g, const Plan &p, DevicePlanTables &out)
 {
-    out.cmask4.assign(p.nsub(), nullptr);
-    out.cmask2.assign(p.nsub(), nullptr);
-    out.cm4_stride.assign(p.nsub(), 0);
-    out.cm2_stride.assign(p.nsub(), 0);
+    out.cmask_f32.assign(p.nsub(), nullptr);
+    out.cmask_f64.assign(p.nsub(), nullptr);
+    out.cmf32_stride.assign(p.nsub(), 0);
+    out.cmf64_stride.assign(p.nsub(), 0);
     out.blk.assign(p.nsub(), nullptr);
     out.blk_shape.assign(p.nsub(), 0);
     out.blk_nblocks.assign(p.nsub(), 0);
@@ -460,8 +460,8 @@ DeviceGraph::~DeviceGraph()
                 for (auto *p : kv.second.aoff) if (p) cudaFreeAsync(p, stream);
                 for (auto *p : kv.second.blk) if (p) cudaFreeAsync(p, stream);
                 for (auto *p : kv.second.moff) if (p) cudaFreeAsync(p, stream);
-                for (auto *p : kv.second.cmask4) if (p) cudaFreeAsync(p, stream);
-                for (auto *p : kv.second.cmask2) if (p) cudaFreeAsync(p, stream);
+                for (auto *p : kv.second.cmask_f32) if (p) cudaFreeAsync(p, stream);
+                for (auto *p : kv.second.cmask_f64) if (p) cudaFreeAsync(p, stream);
             }
             for (auto &kv : it->second.batches) free_batch(kv.second, stream);
             g_state.erase(it);
@@ -673,7 +673,7 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
     if (c.use_adjc) SG_CKS(growT(&w.adjc, &w.adjc_bytes, std::max<size_t>(16, 4 * (size_t)g.nnz), g.stream));
     if (c.hubs.count > 0) {
         // a partial row holds the aux columns (or colour counts) of up to c.lay colorings
-        int32_t maxp = round_up(c.lay * c.p.k, 4);
+        int32_t maxp = round_up(c.lay * c.p.k, 8);
         for (int s : c.p.process_order) {
             const SubTemplate &st = c.p.subs[s];
             const SubTemplate &a = c.p.subs[st.aux];
@@ -754,8 +754,8 @@ StageDesc make_stage(RunCtx &c, int slot, int s, double *root_vertex, int b0 = 0
     d.color = w.colors + (size_t)slot * g.V + b0;
     if (c.use_adjc && slot == 0 && L == 1) {
         d.adjc = w.adjc;
-        d.cmask = c.fp64 ? c.tab->cmask2[s] : c.tab->cmask4[s];
-        d.cmask_stride = c.fp64 ? c.tab->cm2_stride[s] : c.tab->cm4_stride[s];
+        d.cmask = c.fp64 ? c.tab->cmask_f64[s] : c.tab->cmask_f32[s];
+        d.cmask_stride = c.fp64 ? c.tab->cmf64_stride[s] : c.tab->cmf32_stride[s];
     }
     d.off = g.d_off;
     d.adj = g.d_adj;
@@ -1111,7 +1111,7 @@ Status build_batch(RunCtx &c, int slots, bool poison, BatchPlan &bp)
     std::vector<BatchStage> &S = bp.host_stages;
     S.clear();
     int item = 0;
-    size_t smem = (size_t)kBatchThreads * 16;   // hub items' lane partials
+    size_t smem = (size_t)kBatchThreads * 32;   // hub items' lane partials
     for (int s : p.process_order)
         for (int b = 0; b < slots; ++b) {
             void *region = c.hubs.count > 0
@@ -1564,7 +1564,7 @@ Status count_jobs(DeviceGraph &g, const std::vector<const Plan *> &plans, const 
     // one context per job: its plan's device tables, its tables at arena_base
     std::vector<RunCtx> ctx;
     ctx.reserve(n);
-    int32_t hub_pitch = 4;
+    int32_t hub_pitch = 8;
     for (int j = 0; j < n; ++j) {
         const Plan &p = *plans[j];
         ctx.push_back(RunCtx{g, p, gs, nullptr, fp64, es, 0, hubs, 0, 0, o.mode, 0});
@@ -1572,7 +1572,7 @@ Status count_jobs(DeviceGraph &g, const std::vector<const Plan *> &plans, const 
         SG_CKS(make_ctx_tables(g, p, gs, c.tab));
         c.exact = o.exact != 0;
         c.autotune = o.autotune != 0;
-        hub_pitch = std::max<int32_t>(hub_pitch, (int32_t)round_up(p.k, 4));
+        hub_pitch = std::max<int32_t>(hub_pitch, (int32_t)round_up(p.k, 8));
         for (int s : p.process_order) {
             const SubTemplate &a = p.subs[p.subs[s].aux];
             if (a.size > 1) hub_pitch = std::max<int32_t>(hub_pitch, p.table_pitch[p.subs[s].aux]);
@@ -1641,7 +1641,7 @@ Status count_jobs(DeviceGraph &g, const std::vector<const Plan *> &plans, const 
         }
         std::vector<BatchStage> S;
         int item = 0;
-        size_t smem = (size_t)kBatchThreads * 16;
+        size_t smem = (size_t)kBatchThreads * 32;
         for (int lev = 0; lev < maxlev; ++lev)
             for (int j = 0; j < nj; ++j) {
                 RunCtx &c = ctx[j0 + j];

@@ -101,14 +101,14 @@ void launch_remap(int32_t V, const int32_t *old_off, const int32_t *old_adj, con
 template <typename T, int NT, int Q, bool PK>
 __global__ void __launch_bounds__(NT) k_fused(StageDesc d)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(32) unsigned char smem_raw[];
     for (int tile = blockIdx.x; tile < d.ntiles; tile += gridDim.x) fused_tile<T, NT, Q, PK>(d, tile, smem_raw);
 }
 
 template <typename T, int NT>
 __global__ void __launch_bounds__(NT) k_hub(HubArgs h)
 {
-    __shared__ __align__(16) unsigned char smem_raw[NT * 16];
+    __shared__ __align__(32) unsigned char smem_raw[NT * 32];
     for (int item = blockIdx.x; item < h.total_chunks; item += gridDim.x) hub_item<T, NT>(h, item, smem_raw);
 }
 
@@ -122,7 +122,7 @@ bool choose_gather(StageDesc &d, bool fp64, int want = 0)
         d.gather_group = 1;
         return want <= 1;
     }
-    const int CH = fp64 ? 2 : 4;
+    const int CH = fp64 ? 4 : 8;   // elements of a 32-byte chunk
     const int nchunk = (d.aux_cols + CH - 1) / CH;
     const int NT = d.nthreads;
     if (want > 0) {
@@ -170,7 +170,7 @@ bool shape_fits(const StageDesc &d, bool fp64, int tv, int nt, int packed, size_
                  : tile_smem_bytes<float>(La_rows, Lm_rows, oc, tv, packed == 1, d.nb);
     if (bytes > limit) return false;
     if (!d.aux_leaf) {
-        const int CH = fp64 ? 2 : 4;
+        const int CH = fp64 ? 4 : 8;   // elements of a 32-byte chunk
         const int nchunk = (d.aux_cols + CH - 1) / CH;
         if (nchunk > 4 * nt) return false;
     }

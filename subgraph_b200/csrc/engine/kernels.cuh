@@ -39,7 +39,7 @@ void launch_remap(int32_t V, const int32_t *old_off, const int32_t *old_adj, con
 
 struct FusedConfig {
     int tile_v;      // vertices per tile
-    int q;           // 16-byte chunks per gather thread
+    int q;           // 32-byte chunks per gather thread
     size_t smem;     // dynamic shared memory bytes
     int grid;        // CTAs per SM unit (scaled by the occupancy at launch)
 };
@@ -52,7 +52,7 @@ struct TileShape {
     int tile_v;      // vertices per tile
     int threads;     // CTA size
     int packed;      // eMA form: 0 per-output loop, 1 packed FP32x2 (32-vertex tiles), 2 register-blocked
-    int q = 0;       // 16-byte column chunks per aggregation thread (1, 2, 4); 0: the fewest that keep
+    int q = 0;       // 32-byte column chunks per aggregation thread (1, 2, 4); 0: the fewest that keep
                      // nine in ten threads busy
 };
 // Sets an explicit shape (the autotuner's candidates); false when it does not fit.

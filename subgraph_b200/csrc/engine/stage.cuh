@@ -12,7 +12,7 @@ enum CountMode : int32_t {
 
 // One sub-template step of nb colorings: the fused aggregation + eMA over all
 // vertices.  Tables are vertex-major: row v holds the v-th vertex's L columns
-// with a pitch that is a multiple of 4 elements (16 B for FP32).  A batch of
+// with a pitch that is a multiple of 8 elements (32-byte rows).  A batch of
 // B colorings interleaves them per vertex: row v = [B][pitch] (row stride
 // B*pitch), colors [V][B]; a launch handles colorings [b0, b0 + nb) of it
 // (the table and color pointers are offset to b0).  The plain form is
@@ -36,7 +36,7 @@ struct StageDesc {
     int32_t tile_v;                    // vertices per tile
     int32_t nthreads;                  // CTA size (256 or 512)
     int32_t gather_group;              // threads per vertex in the aggregation
-    int32_t gather_q;                  // 16-byte column chunks per thread (1, 2 or 4)
+    int32_t gather_q;                  // 32-byte column chunks per thread (1, 2 or 4)
     int32_t ntiles;
     int32_t out_chunk;                 // outputs staged in shared memory per pass
     size_t smem;                       // dynamic shared memory bytes
@@ -67,7 +67,7 @@ struct StageDesc {
     // meet a main entry that is an exact zero, or no output at all), and a
     // neighbour of color c_u only adds to sets containing c_u (its other
     // entries are exact zeros): cmask[c][chunk] has bit c_u set when the
-    // 16-byte column chunk holds such a set; other chunks are skipped.
+    // 32-byte column chunk holds such a set; other chunks are skipped.
     const int32_t *adjc;               // [nnz], or null (adj)
     const uint16_t *cmask;             // [k][cmask_stride] (with adjc, non-leaf aux), or null: every chunk read
     int32_t cmask_stride;

@@ -34,23 +34,44 @@ __device__ __forceinline__ float leaf_value(float agg, bool scaled)
 }
 __device__ __forceinline__ double leaf_value(double agg, bool) { return agg; }
 
+// 32-byte column chunks of table rows (rows are 32-byte aligned: pitches are
+// multiples of 8 elements), loaded with one 256-bit load each.
+struct __align__(32) F8 { float v[8]; };
+struct __align__(32) D4 { double v[4]; };
 template <typename T> struct Chunk;
 template <> struct Chunk<float> {
-    using type = float4;
-    static constexpr int n = 4;
-    __device__ static float get(const float4 &v, int i) { return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w; }
-    __device__ static void add(float4 &a, const float4 &b)
+    using type = F8;
+    static constexpr int n = 8;
+    __device__ static float get(const F8 &c, int i) { return c.v[i]; }
+    __device__ static void add(F8 &a, const F8 &b)
     {
-        a.x = __fadd_rn(a.x, b.x); a.y = __fadd_rn(a.y, b.y); a.z = __fadd_rn(a.z, b.z); a.w = __fadd_rn(a.w, b.w);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) a.v[i] = __fadd_rn(a.v[i], b.v[i]);
     }
-    __device__ static float4 zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+    __device__ static F8 zero()
+    {
+        F8 z;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) z.v[i] = 0.f;
+        return z;
+    }
 };
 template <> struct Chunk<double> {
-    using type = double2;
-    static constexpr int n = 2;
-    __device__ static double get(const double2 &v, int i) { return i == 0 ? v.x : v.y; }
-    __device__ static void add(double2 &a, const double2 &b) { a.x = __dadd_rn(a.x, b.x); a.y = __dadd_rn(a.y, b.y); }
-    __device__ static double2 zero() { return make_double2(0.0, 0.0); }
+    using type = D4;
+    static constexpr int n = 4;
+    __device__ static double get(const D4 &c, int i) { return c.v[i]; }
+    __device__ static void add(D4 &a, const D4 &b)
+    {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a.v[i] = __dadd_rn(a.v[i], b.v[i]);
+    }
+    __device__ static D4 zero()
+    {
+        D4 z;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) z.v[i] = 0.0;
+        return z;
+    }
 };
 
 // Loads of count tables and partial rows.  The per-stage kernels read tables
@@ -58,6 +79,34 @@ template <> struct Chunk<double> {
 // path); the persistent kernel reads tables produced inside the same launch,
 // so it loads them through L2 (ld.global.cg), the point of coherence.
 template <bool COH, typename P> __device__ __forceinline__ P ld_tab(const P *p) { return COH ? __ldcg(p) : __ldg(p); }
+// 256-bit chunk loads: non-coherent (read-only for the launch), or through L2
+template <bool COH> __device__ __forceinline__ F8 ld_tab(const F8 *p)
+{
+    F8 r;
+    if (COH)
+        asm volatile("ld.global.cg.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]), "=f"(r.v[4]), "=f"(r.v[5]), "=f"(r.v[6]),
+                       "=f"(r.v[7])
+                     : "l"(p)
+                     : "memory");
+    else
+        asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+            : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]), "=f"(r.v[4]), "=f"(r.v[5]), "=f"(r.v[6]), "=f"(r.v[7])
+            : "l"(p));
+    return r;
+}
+template <bool COH> __device__ __forceinline__ D4 ld_tab(const D4 *p)
+{
+    D4 r;
+    if (COH)
+        asm volatile("ld.global.cg.v4.f64 {%0,%1,%2,%3}, [%4];"
+                     : "=d"(r.v[0]), "=d"(r.v[1]), "=d"(r.v[2]), "=d"(r.v[3])
+                     : "l"(p)
+                     : "memory");
+    else
+        asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(r.v[0]), "=d"(r.v[1]), "=d"(r.v[2]), "=d"(r.v[3]) : "l"(p));
+    return r;
+}
 
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
@@ -117,7 +166,7 @@ __device__ __forceinline__ unsigned long long add2_rn(unsigned long long a, unsi
 // One tile of one stage: TV consecutive (degree-ordered) vertices.
 //   A. aggregation of the aux child's rows over each vertex's neighbours into
 //      shared memory, transposed [column][vertex]: `gather_group` threads per
-//      vertex, each owning gather_q 16-byte column chunks, neighbour ids and
+//      vertex, each owning gather_q 32-byte column chunks, neighbour ids and
 //      rows fetched in batches of U before they are added (memory-level
 //      parallelism without reordering the sums).  A one-hot aux child becomes
 //      a per-color neighbour count.  Hub vertices add their partial rows.
@@ -136,7 +185,8 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
     using C = typename CT::type;
     constexpr int CH = CT::n;
     constexpr int NW = NT / 32;
-    constexpr int U = Q == 1 ? 8 : (Q == 2 ? 4 : 2);
+    // neighbours per batch: 128 bytes of row chunks in flight per thread
+    constexpr int U = 128 / (Q * (int)sizeof(C)) > 0 ? 128 / (Q * (int)sizeof(C)) : 1;
     const int TV = d.tile_v;
     const int TVP = TV + 1;
     const int RS = PK ? kPackedRow : TVP;          // row stride of the aggregate and main rows
@@ -565,7 +615,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
 // partial row.  Threads are (neighbour lane r, column chunk q); lane r sums
 // the chunk's neighbours r, r+R, ... in order, and the R lane sums are added
 // in lane order: a fixed summation order.  A one-hot aux child counts colors.
-// Needs NT * 16 bytes of shared memory (the lane partials).
+// Needs NT * 32 bytes of shared memory (the lane partials), 32-byte aligned.
 // ---------------------------------------------------------------------------
 template <typename T, int NT, bool COH = false>
 __device__ __forceinline__ void hub_item(const HubArgs &h, int item, unsigned char *smem_raw)

@@ -305,7 +305,7 @@ bool make_plan(const Template &t, Plan &p, std::string &err)
     for (int si : p.process_order) {
         SubTemplate &s = p.subs[si];
         if (si > 0) {
-            p.table_pitch[si] = (s.L + 3) / 4 * 4;
+            p.table_pitch[si] = (s.L + 7) / 8 * 8;   // 32-byte rows for the 256-bit aggregation loads
             p.table_offset[si] = alloc(p.table_pitch[si]);
             peak = std::max(peak, top);
         }
