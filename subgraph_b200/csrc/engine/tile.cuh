@@ -74,6 +74,25 @@ template <> struct Chunk<double> {
     }
 };
 
+// 16-byte chunks for the hub items, whose threads split the chunk's
+// neighbours as well as its columns: narrower chunks give more of them.
+template <typename T> struct Chunk16;
+template <> struct Chunk16<float> {
+    using type = float4;
+    static constexpr int n = 4;
+    __device__ static void add(float4 &a, const float4 &b)
+    {
+        a.x = __fadd_rn(a.x, b.x); a.y = __fadd_rn(a.y, b.y); a.z = __fadd_rn(a.z, b.z); a.w = __fadd_rn(a.w, b.w);
+    }
+    __device__ static float4 zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+};
+template <> struct Chunk16<double> {
+    using type = double2;
+    static constexpr int n = 2;
+    __device__ static void add(double2 &a, const double2 &b) { a.x = __dadd_rn(a.x, b.x); a.y = __dadd_rn(a.y, b.y); }
+    __device__ static double2 zero() { return make_double2(0.0, 0.0); }
+};
+
 // Loads of count tables and partial rows.  The per-stage kernels read tables
 // written by earlier launches (read-only for the launch: the non-coherent
 // path); the persistent kernel reads tables produced inside the same launch,
@@ -620,7 +639,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
 template <typename T, int NT, bool COH = false>
 __device__ __forceinline__ void hub_item(const HubArgs &h, int item, unsigned char *smem_raw)
 {
-    using CT = Chunk<T>;
+    using CT = Chunk16<T>;
     using C = typename CT::type;
     constexpr int CH = CT::n;
     int lo = 0, hi = h.hub_count - 1;
