@@ -62,7 +62,8 @@ WORKLOADS = {
 # a seeded stream of 256 jobs, each a random tree of 3-10 vertices (uniform
 # Pruefer sequence, smallest-leaf decoding, edges in decode order) on one of
 # three R-MAT graphs (scales 16, 18, 20, edge factor 8): one coloring per job,
-# the jobs of a graph in persistent job-queue launches
+# the jobs of a graph spread over CUDA streams (--persistent: one persistent
+# job-queue launch per graph and wave)
 MIXED = dict(jobs=256, stream_seed=5, scales=(16, 18, 20), ef=8, seed=7)
 WORKLOADS["mixed256_rmat16_18_20_ef8"] = dict(mixed=True, per_step=MIXED["jobs"], template="random 3-10",
                                               scale="16/18/20", ef=8, seed=7)
@@ -229,7 +230,8 @@ def run_mixed(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     cfg = {"workload": args.workload, "jobs": MIXED["jobs"], "templates": "random trees of 3-10 vertices",
            "graphs": "rmat scales 16/18/20 edge factor 8 seed 1", "stream_seed": MIXED["stream_seed"],
-           "form": "persistent job queue per graph", "tables": "fp32", "sums": "fp64",
+           "form": ("persistent job queue per graph" if args.persistent
+                    else f"job streams per graph ({args.batch or 8} CUDA streams)"), "tables": "fp32", "sums": "fp64",
            "l2": "inputs larger than L2 at scales 18 and 20"}
     graphs = []
     for sc in MIXED["scales"]:
@@ -274,7 +276,8 @@ def run_mixed(args):
             if not idx:
                 continue
             r, l, st = sg.count_jobs(dgs[gi], [tmpls[j] for j in idx], [jobs[j][3] for j in idx],
-                                     return_latency=True, return_stats=True)
+                                     return_latency=True, return_stats=True, persistent=args.persistent,
+                                     streams=args.batch)
             raw[idx], lat[idx] = r, l + ms   # the graphs run one after the other
             ms += st["device_ms"]
         return ms, lat, raw
@@ -306,7 +309,7 @@ def run_mixed(args):
     for _ in range(args.steps):
         for gi, idx in enumerate(by_graph):
             ts = [sg.Graph(jobs[j][1], jobs[j][2]) for j in idx]
-            sg.count_jobs(dgs[gi], ts, [jobs[j][3] for j in idx])
+            sg.count_jobs(dgs[gi], ts, [jobs[j][3] for j in idx], persistent=args.persistent, streams=args.batch)
     e2e_s = time.perf_counter() - t0
     line = {"metric": METRIC, "value": value, "unit": "colorings/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot / args.steps, "higher_is_better": True, "scaling": "weak",

@@ -184,11 +184,16 @@ void sg_count_opts_default(sg_count_opts *o);
 sg_status sg_count(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw, sg_count_stats *stats);
 
 /* A stream of jobs with different templates on one graph: job j counts one
- * coloring of plans[j] seeded srand(seeds[j]) into raw[j].  The jobs run as
- * persistent work-queue launches (all their sub-template stages in one queue,
- * waves admitted by free device memory).  From opts: mode, hub_threshold,
- * exact, wait_limit_ms, no_autotune.  job_ms (optional, n_jobs): each job's latency from
- * the start of its wave's launch to the end of its last stage.  The reference
+ * coloring of plans[j] seeded srand(seeds[j]) into raw[j].  Default form: the
+ * jobs' stage launches (those of sg_count) are spread over opts.batch CUDA
+ * streams (0: 8; fewer when device memory is short), each stream with its own
+ * table slot, so the launches of different jobs overlap.  opts.persistent = 1:
+ * the jobs run as persistent work-queue launches instead (all their
+ * sub-template stages in one queue, waves admitted by free device memory).
+ * From opts also: mode, hub_threshold, exact, wait_limit_ms, no_autotune,
+ * no_blocked.  job_ms (optional, n_jobs): each job's latency from the start of
+ * the call's launches (stream form) or of its wave's launch (persistent form)
+ * to the end of its last stage.  The reference
  * runs one template per CountMat::compute (CountMat.cpp:79-266); this is the
  * batched mixed-template form with no single counterpart there. */
 sg_status sg_count_jobs(sg_graph g, int32_t n_jobs, const sg_plan *plans, const uint32_t *seeds,

@@ -467,10 +467,13 @@ def count(graph: DeviceGraph, template: Graph, n_colorings: int = 1, seed_base: 
 
 
 def count_jobs(graph: DeviceGraph, templates, seeds, mode: int = MODE_REFERENCE, hub_threshold: int = 1024,
-               exact: bool = False, wait_limit_ms: int = 0, return_latency: bool = False, return_stats: bool = False):
+               exact: bool = False, wait_limit_ms: int = 0, return_latency: bool = False, return_stats: bool = False,
+               persistent: bool = False, streams: int = 0):
     """One coloring each of jobs with different templates on one graph (job j:
-    templates[j] seeded srand(seeds[j])), in persistent work-queue launches.
-    Returns the raw counts; with return_latency also each job's latency (ms)."""
+    templates[j] seeded srand(seeds[j])): their stage launches spread over
+    `streams` CUDA streams (0: 8), or with persistent=True in persistent
+    work-queue launches.  Returns the raw counts; with return_latency also each
+    job's latency (ms)."""
     n = len(templates)
     if n != len(seeds):
         raise ValueError("one seed per job")
@@ -482,6 +485,8 @@ def count_jobs(graph: DeviceGraph, templates, seeds, mode: int = MODE_REFERENCE,
     o.hub_threshold = hub_threshold
     o.exact = 1 if exact else 0
     o.wait_limit_ms = wait_limit_ms
+    o.persistent = 1 if persistent else 0
+    o.batch = streams
     raw = np.zeros(n, np.float64)
     lat = np.zeros(n, np.float64)
     st = CountStats()

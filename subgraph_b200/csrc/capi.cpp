@@ -403,6 +403,9 @@ sg_status sg_count_jobs(sg_graph g, int32_t n_jobs, const sg_plan *plans, const 
     co.exact = o->exact ? 1 : 0;
     co.wait_limit_ms = o->wait_limit_ms;
     co.autotune = o->no_autotune ? 0 : 1;
+    co.persistent = o->persistent ? 1 : 0;
+    co.batch = o->batch;
+    co.blocked = o->no_blocked ? 0 : 1;
     sg::CountStats cs;
     sg_status st = from(sg::count_jobs(*g->g, ps, seeds, co, raw, job_ms, &cs));
     if (st) return st;

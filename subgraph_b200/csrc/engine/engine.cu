@@ -146,6 +146,7 @@ struct GraphState {
     Workspace ws;
     std::map<uint64_t, DevicePlanTables> plans;
     std::map<std::string, BatchPlan> batches; // batch shape -> work queue
+    std::vector<cudaStream_t> streams;        // job streams (created on first use)
 };
 
 std::string shape_key(const StageDesc &d, bool fp64, int hubs)
@@ -464,6 +465,10 @@ DeviceGraph::~DeviceGraph()
                 for (auto *p : kv.second.cmask_f64) if (p) cudaFreeAsync(p, stream);
             }
             for (auto &kv : it->second.batches) free_batch(kv.second, stream);
+            for (cudaStream_t js : it->second.streams) {
+                cudaStreamSynchronize(js);
+                cudaStreamDestroy(js);
+            }
             g_state.erase(it);
         }
     }
@@ -604,7 +609,8 @@ struct RunCtx {
     int lay = 1;             // colorings interleaved per table row (grouped batched form)
     size_t arena_base = 0;   // byte offset of this context's tables in the arena (job queues)
     bool exact = false;      // no fused products (packed eMA), no hub chunks
-    bool use_adjc = false;   // one coloring at a time in slot 0: neighbour ids carry their colors
+    bool use_adjc = false;   // one coloring at a time per slot: neighbour ids carry their colors
+    void *hub_region = nullptr;  // this context's hub partial rows (job streams), else the workspace's
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> fused_ev, hub_ev;
     std::vector<std::pair<int, double>> fused_sub;   // per fused launch: sub, compulsory bytes
     double fused_alg_bytes = 0, fused_gather_bytes = 0;
@@ -752,8 +758,8 @@ StageDesc make_stage(RunCtx &c, int slot, int s, double *root_vertex, int b0 = 0
     d.blk_shape = d.blk ? c.tab->blk_shape[s] : 0;
     d.blk_nblocks = d.blk ? c.tab->blk_nblocks[s] : 0;
     d.color = w.colors + (size_t)slot * g.V + b0;
-    if (c.use_adjc && slot == 0 && L == 1) {
-        d.adjc = w.adjc;
+    if (c.use_adjc && L == 1) {
+        d.adjc = w.adjc + (size_t)slot * g.nnz;
         d.cmask = c.fp64 ? c.tab->cmask_f64[s] : c.tab->cmask_f32[s];
         d.cmask_stride = c.fp64 ? c.tab->cmf64_stride[s] : c.tab->cmf32_stride[s];
     }
@@ -798,7 +804,7 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
     DeviceGraph &g = c.g;
     StageDesc d = make_stage(c, slot, s, root_vertex, b0, nb);
     if (c.hubs.count > 0) {
-        HubArgs h = make_hub(c, d, c.gs.ws.hub_partial);
+        HubArgs h = make_hub(c, d, c.hub_region ? c.hub_region : c.gs.ws.hub_partial);
         if (c.profile) {
             SG_CKS(ev_pair(c.hub_ev));
             SG_CK(cudaEventRecord(c.hub_ev.back().first, st));
@@ -901,8 +907,9 @@ Status launch_colors(RunCtx &c, int slot0, int first_coloring, int n, cudaStream
     a.vertex_stride = c.lay;
     launch_color(a, n, st);
     c.launches += 1;
-    if (c.use_adjc && c.lay == 1 && slot0 == 0 && n == 1) {
-        launch_color_adj(c.g.d_adj, c.g.nnz, c.gs.ws.colors, c.gs.ws.adjc, st);
+    if (c.use_adjc && c.lay == 1 && n == 1) {
+        launch_color_adj(c.g.d_adj, c.g.nnz, c.gs.ws.colors + (size_t)slot0 * c.g.V, c.gs.ws.adjc + (size_t)slot0 * c.g.nnz,
+                         st);
         c.launches += 1;
     }
     SG_CK(cudaGetLastError());
@@ -1542,9 +1549,13 @@ namespace sg {
 // earlier stages of its own job.  The CTA that completes a job's root stage
 // stamps %globaltimer, which gives each job's latency from the launch start.
 // ---------------------------------------------------------------------------
+Status count_jobs_streams(DeviceGraph &g, const std::vector<const Plan *> &plans, const uint32_t *seeds,
+                          const CountOptions &o, double *raw, double *job_ms, CountStats *stats);
+
 Status count_jobs(DeviceGraph &g, const std::vector<const Plan *> &plans, const uint32_t *seeds,
                   const CountOptions &o, double *raw, double *job_ms, CountStats *stats)
 {
+    if (!o.persistent) return count_jobs_streams(g, plans, seeds, o, raw, job_ms, stats);
     const int n = (int)plans.size();
     if (n < 1) return Status{1, "no jobs"};
     if (!seeds || !raw) return Status{1, "null argument"};
@@ -1710,6 +1721,145 @@ Status count_jobs(DeviceGraph &g, const std::vector<const Plan *> &plans, const 
         stats->device_ms = total_ms;
         stats->kernel_launches = launches;
         stats->table_bytes = (int64_t)w.arena_bytes;
+    }
+    return Status::ok();
+}
+
+// ---------------------------------------------------------------------------
+// Job streams, stream form: every job runs the plain form's tuned stage
+// launches (register-blocked eMA, colour-tagged neighbours, chunk masks) on
+// one of S CUDA streams; stream s owns table slot s (the largest job's arena),
+// its colors, colour-tagged adjacency, root partials and hub rows, and takes
+// jobs s, s+S, ... in order, so slots are reused only by later jobs of the
+// same stream.  The launches of different streams overlap on the GPU, which
+// fills it when one job's launches are short.  Each job's latency is the
+// time from the common start event to the end of its root sum.
+// ---------------------------------------------------------------------------
+Status count_jobs_streams(DeviceGraph &g, const std::vector<const Plan *> &plans, const uint32_t *seeds,
+                          const CountOptions &o, double *raw, double *job_ms, CountStats *stats)
+{
+    const int n = (int)plans.size();
+    if (n < 1) return Status{1, "no jobs"};
+    if (!seeds || !raw) return Status{1, "null argument"};
+    if (o.mode < 0 || o.mode > 2) return Status{1, "unknown count mode"};
+    for (const Plan *p : plans)
+        if (!p) return Status{1, "null template plan"};
+    if (g.V >= (1 << 28)) return Status{1, "counting supports graphs of fewer than 2^28 vertices"};
+    SG_CK(cudaSetDevice(g.device));
+    GraphState &gs = state_of(g);
+    Workspace &w = gs.ws;
+    const bool fp64 = o.mode == kModeFP64;
+    const size_t es = fp64 ? 8 : 4;
+    const size_t V = (size_t)g.V;
+    cudaStream_t st = g.stream;
+    const Hubs hubs = plan_hubs(g, o.exact ? 0 : o.hub_threshold);
+    std::vector<RunCtx> ctx;
+    ctx.reserve(n);
+    size_t max_arena = 16;
+    int32_t hub_pitch = 8;
+    for (int j = 0; j < n; ++j) {
+        const Plan &p = *plans[j];
+        ctx.push_back(RunCtx{g, p, gs, nullptr, fp64, es, 0, hubs, 0, 0, o.mode, 0});
+        RunCtx &c = ctx.back();
+        SG_CKS(make_ctx_tables(g, p, gs, c.tab));
+        c.exact = o.exact != 0;
+        c.autotune = o.autotune != 0;
+        c.blocked = o.blocked != 0;
+        c.use_adjc = adjc_ok(g, p);
+        max_arena = std::max(max_arena, (size_t)p.arena_units * V * es);
+        hub_pitch = std::max<int32_t>(hub_pitch, (int32_t)round_up(p.k, 8));
+        for (int s : p.process_order)
+            if (p.subs[p.subs[s].aux].size > 1) hub_pitch = std::max<int32_t>(hub_pitch, p.table_pitch[p.subs[s].aux]);
+    }
+    const bool adjc = ctx[0].use_adjc;
+    const size_t hub_region = (size_t)hubs.total_chunks * (size_t)hub_pitch * es;
+    // streams admitted by free memory: a slot holds one job's tables, colors,
+    // colour-tagged adjacency, root partials and hub rows
+    int S = std::max(1, std::min(o.batch > 0 ? o.batch : 8, n));
+    {
+        size_t free_b = 0, total_b = 0;
+        SG_CK(cudaMemGetInfo(&free_b, &total_b));
+        const size_t per = max_arena + V + 8 * (V / 8 + 2) + hub_region + (adjc ? 4 * (size_t)g.nnz : 0);
+        const size_t have = w.arena_bytes + w.hub_partial_bytes + w.adjc_bytes;
+        while (S > 1 && per * (size_t)S > (size_t)((double)(free_b + have) * 0.85)) --S;
+    }
+    SG_CKS(grow(&w.arena, &w.arena_bytes, max_arena * S, st));
+    SG_CKS(growT(&w.colors, &w.colors_bytes, std::max<size_t>(16, V * S), st));
+    SG_CKS(growT(&w.partial, &w.partial_bytes, 8 * (V / 8 + 2) * S, st));
+    SG_CKS(growT(&w.raw, &w.raw_bytes, 8 * (size_t)n, st));
+    SG_CKS(growT(&w.windows, &w.windows_bytes, 4 * 31 * (size_t)n, st));
+    if (adjc) SG_CKS(growT(&w.adjc, &w.adjc_bytes, std::max<size_t>(16, 4 * (size_t)g.nnz * S), st));
+    if (hubs.count > 0) {
+        SG_CKS(grow(&w.hub_partial, &w.hub_partial_bytes, std::max<size_t>(16, hub_region * S), st));
+        std::vector<int32_t> cs((size_t)hubs.count + 1, 0);
+        for (int h = 0; h < hubs.count; ++h) cs[h + 1] = cs[h] + (g.h_degree[h] + hubs.chunk - 1) / hubs.chunk;
+        SG_CKS(growT(&w.chunk_start, &w.chunk_start_bytes, 4 * cs.size(), st));
+        SG_CK(cudaMemcpyAsync(w.chunk_start, cs.data(), 4 * cs.size(), cudaMemcpyHostToDevice, st));
+        SG_CK(cudaStreamSynchronize(st));   // `cs` is pageable and goes out of scope
+    }
+    {
+        std::vector<uint32_t> win((size_t)n * 31);
+        for (int j = 0; j < n; ++j) glibc_window(seeds[j], &win[(size_t)j * 31]);
+        SG_CK(cudaMemcpyAsync(w.windows, win.data(), win.size() * 4, cudaMemcpyHostToDevice, st));
+        SG_CK(cudaStreamSynchronize(st));
+    }
+    while ((int)gs.streams.size() < S) {
+        cudaStream_t js;
+        SG_CK(cudaStreamCreateWithFlags(&js, cudaStreamNonBlocking));
+        gs.streams.push_back(js);
+    }
+    for (RunCtx &c : ctx) {
+        c.arena_per_coloring = max_arena;
+        c.hub_pitch = hub_pitch;
+    }
+    std::vector<cudaEvent_t> ev_end(n, nullptr);
+    cudaEvent_t ev0;
+    SG_CK(cudaEventCreate(&ev0));
+    for (int j = 0; j < n; ++j) SG_CK(cudaEventCreate(&ev_end[j]));
+    SG_CK(cudaEventRecord(ev0, st));
+    for (int s = 0; s < S; ++s) SG_CK(cudaStreamWaitEvent(gs.streams[s], ev0, 0));
+    const double scale = o.mode == kModeReference ? 1.0e12 : 1.0;
+    int64_t launches = 0;
+    Status status = Status::ok();
+    for (int j = 0; j < n && !status.code; ++j) {
+        const int s = j % S;
+        cudaStream_t js = gs.streams[s];
+        RunCtx &c = ctx[j];
+        c.hub_region = hubs.count > 0 ? (char *)w.hub_partial + hub_region * s : nullptr;
+        status = launch_colors(c, s, j, 1, js);
+        for (int sub : c.p.process_order)
+            if (!status.code) status = run_stage(c, s, sub, nullptr, js);
+        if (status.code) break;
+        launch_root_reduce(w.partial + (size_t)s * (V / 8 + 2), c.root_tiles, scale, w.raw + j, js);
+        cudaEventRecord(ev_end[j], js);
+        launches += c.launches + 1;
+    }
+    // join: the default stream waits for every job stream
+    for (int s = 0; s < S; ++s) {
+        cudaEvent_t e;
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess) {
+            cudaEventRecord(e, gs.streams[s]);
+            cudaStreamWaitEvent(st, e, 0);
+            cudaEventDestroy(e);
+        }
+    }
+    if (!status.code) SG_CK(cudaMemcpyAsync(raw, w.raw, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    SG_CK(cudaStreamSynchronize(st));
+    double total = 0;
+    for (int j = 0; j < n; ++j) {
+        float ms = 0;
+        if (!status.code && cudaEventElapsedTime(&ms, ev0, ev_end[j]) == cudaSuccess) {
+            if (job_ms) job_ms[j] = ms;
+            total = std::max(total, (double)ms);
+        }
+        cudaEventDestroy(ev_end[j]);
+    }
+    cudaEventDestroy(ev0);
+    if (status.code) return status;
+    if (stats) {
+        stats->device_ms = total;
+        stats->kernel_launches = launches;
+        stats->table_bytes = (int64_t)(max_arena * S);
     }
     return Status::ok();
 }
