@@ -856,8 +856,9 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
                 c.launches += 3;
                 if (ms < best) { best = ms; pick = cand; }
                 if (std::getenv("SG_TUNE_LOG"))
-                    std::fprintf(stderr, "[sg tune] sub %d shape %s tile %d threads %d packed %d q %d group %d: %.3f ms\n",
-                                 s, key.c_str(), cand.tile_v, cand.threads, cand.packed, dc.gather_q, dc.gather_group, ms);
+                    std::fprintf(stderr, "[sg tune] sub %d shape %s tile %d threads %d packed %d q %d group %d mask %d: %.3f ms\n",
+                                 s, key.c_str(), cand.tile_v, cand.threads, cand.packed, dc.gather_q, dc.gather_group,
+                                 dc.cmask ? 1 : 0, ms);
             }
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);

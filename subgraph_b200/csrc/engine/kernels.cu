@@ -188,6 +188,7 @@ bool set_shape(StageDesc &d, bool fp64, const TileShape &sh)
     d.out_chunk = oc;
     d.smem = bytes;
     d.ntiles = (d.V + sh.tile_v - 1) / sh.tile_v;
+    if (sh.nomask) d.cmask = nullptr;
     return choose_gather(d, fp64, sh.q);
 }
 
@@ -210,6 +211,14 @@ std::vector<TileShape> candidate_shapes(const StageDesc &d, bool fp64)
         int oc;
         if (!shape_fits(d, fp64, c.tile_v, c.threads, c.packed, 227 * 1024, bytes, oc)) continue;
         out.push_back(c);
+        // with chunk masks: also without them (the masks save loads but not the
+        // instructions around them)
+        if (d.cmask && !c.nomask) {
+            TileShape t = c;
+            t.nomask = 1;
+            StageDesc f = d;
+            if (set_shape(f, fp64, t)) out.push_back(t);
+        }
         // wide aggregations: also the other chunk counts per thread (more chunks
         // per thread share one neighbour id and row address among them)
         if (!d.aux_leaf && d.aux_cols >= 64) {

@@ -54,6 +54,7 @@ struct TileShape {
     int packed;      // eMA form: 0 per-output loop, 1 packed FP32x2 (32-vertex tiles), 2 register-blocked
     int q = 0;       // 32-byte column chunks per aggregation thread (1, 2, 4); 0: the fewest that keep
                      // nine in ten threads busy
+    int nomask = 0;  // 1: read every column chunk (no chunk masks)
 };
 // Sets an explicit shape (the autotuner's candidates); false when it does not fit.
 bool set_shape(StageDesc &d, bool fp64, const TileShape &shape);
