@@ -305,12 +305,18 @@ bool make_plan(const Template &t, Plan &p, std::string &err)
     for (int si : p.process_order) {
         SubTemplate &s = p.subs[si];
         if (si > 0) {
-            p.table_pitch[si] = (s.L + 7) / 8 * 8;   // 32-byte rows for the 256-bit aggregation loads
-            p.table_offset[si] = alloc(p.table_pitch[si]);
+            // rows an aggregation gathers (the parent's aux child) are 32-byte
+            // aligned for its 256-bit loads; main-child rows, read element by
+            // element, keep 16-byte rows
+            const bool gathered = s.parent >= 0 && s.parent < ns && p.subs[s.parent].aux == si;
+            p.table_pitch[si] = gathered ? (s.L + 7) / 8 * 8 : (s.L + 3) / 4 * 4;
+            // arena slots are whole multiples of 8 units, so every table starts
+            // 32-byte aligned for any V
+            p.table_offset[si] = alloc((p.table_pitch[si] + 7) / 8 * 8);
             peak = std::max(peak, top);
         }
         for (int c : {s.main, s.aux})
-            if (p.subs[c].size > 1) release(p.table_offset[c], p.table_pitch[c]);
+            if (p.subs[c].size > 1) release(p.table_offset[c], (p.table_pitch[c] + 7) / 8 * 8);
     }
     p.arena_units = peak;
     p.automorphisms = 1;

@@ -44,7 +44,7 @@ struct Plan {
 
     // count-table arena, in units of "V elements" (a table of pitch P uses P units)
     std::vector<int64_t> table_offset;   // per sub, -1 when the sub has no table
-    std::vector<int32_t> table_pitch;    // row pitch (elements), multiple of 8
+    std::vector<int32_t> table_pitch;    // row pitch (elements): multiple of 8 for aux children, else of 4
     int64_t arena_units = 0;
 
     int nsub() const { return (int)subs.size(); }
