@@ -206,3 +206,19 @@ def test_text_round_trip(tmp_path):
     el2 = sg.EdgeList(p)
     assert el2.getNumVertices() == el.getNumVertices()
     assert np.array_equal(el2.getSrcList(), el.getSrcList())
+
+
+def test_table_arena_slots_keep_32_byte_rows():
+    """The aggregation reads gathered tables with 256-bit loads, so every table
+    must start 32-byte aligned for any vertex count: the arena of every plan
+    is a whole number of 8-unit slots (a unit is V elements)."""
+    import ctypes
+    from subgraph_b200._lib import lib
+    rng = random.Random(29)
+    trees = [TEMPLATES[t] for t in ("p3", "tree5", "spider7", "tree12")]
+    trees += [(n, prufer_tree(n, rng)) for n in (rng.randint(3, 16) for _ in range(60))]
+    for n, edges in trees:
+        g = sg.Graph(n, edges)
+        units = ctypes.c_int64()
+        assert lib().sg_plan_info(g.plan, None, None, None, ctypes.byref(units)) == 0
+        assert units.value > 0 and units.value % 8 == 0, (n, edges, units.value)
