@@ -269,6 +269,8 @@ def run_mixed(args):
     tmpls = [sg.Graph(n, e) for _, n, e, _ in jobs]
     by_graph = [[j for j, job in enumerate(jobs) if job[0] == gi] for gi in range(len(graphs))]
 
+    launches = [0]
+
     def step():
         ms, lat = 0.0, np.zeros(len(jobs))
         raw = np.zeros(len(jobs))
@@ -280,11 +282,13 @@ def run_mixed(args):
                                      streams=args.batch)
             raw[idx], lat[idx] = r, l + ms   # the graphs run one after the other
             ms += st["device_ms"]
+            launches[0] += st["kernel_launches"]
         return ms, lat, raw
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    launches[0] = 0
     tot, lats = 0.0, []
     with Clocks(local) as clk:
         torch.cuda.nvtx.range_push("timed")
@@ -316,7 +320,7 @@ def run_mixed(args):
             "vs_baseline": None, "dtype": "fp32", "data": "synthetic", "config": cfg,
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "forms": {"plain": plain, "batched": value, "batched_over_plain": value / plain, "unit": "colorings/s"},
-            "roofline": None, "gpu_launches": None, "clocks": clocks,
+            "roofline": None, "gpu_launches": launches[0], "clocks": clocks,
             "e2e": {"value": world * len(jobs) * args.steps / e2e_s, "unit": "colorings/s",
                     "h2d_bytes_per_step": 124 * len(jobs),   # one 31-word coloring window per job
                     "d2h_bytes_per_step": 16 * len(jobs)}}
