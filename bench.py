@@ -13,10 +13,15 @@ tables, 16 colorings per step (coloring c seeded srand(7 + c)).
             region), all colorings counted, raw counts read back (D2H).
   roofline  the fused aggregation+eMA kernel: compulsory bytes per launch
             divided by its CUDA-event duration, against MEASURED_PEAKS.json.
-  cpu_baseline  the reference's own CPU code (oracle/_ref/sc-nec-ncc.bin,
-            built from the reference sources) on the host cores.
+  cpu_baseline  the reference's own CPU code (its CountMat::colorCounting,
+            built from the reference sources into oracle/_ref/) on the host
+            cores, on the first two colorings the GPU timed, same graph: its
+            raw counts give rel_err_vs_reference.
 
---impl reference runs that reference binary alone (rank 0) and prints its line.
+--impl reference runs the reference's stock CLI (oracle/_ref/sc-nec-ncc.bin)
+alone on rank 0 on the same text edge list (one coloring per step) and prints
+its line.  The graphs are written by subgraph_b200.synth (numpy only), so
+that arm never loads this project's library.
 Multi-GPU (torchrun): every rank counts its own colorings of the same graph
 (independent replicas, weak scaling); the only exchange is the max of the
 step times and a gather of the counts.
@@ -161,59 +166,93 @@ class Clocks:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def graph_file(scale: int, ef: int) -> str:
+    """The workload's R-MAT graph as a text edge list (numpy generator, cached)."""
+    from subgraph_b200 import synth
+    return synth.rmat_file(scale, ef, seed=1)
+
+
 def build_graph(w):
+    """Host CSC of the workload's graph, read from its text file by the
+    library's EdgeList (EdgeList.cpp:34-116 semantics)."""
     import subgraph_b200 as sg
-    el = sg.rmat(w["scale"], w["ef"], seed=1)
+    path = graph_file(w["scale"], w["ef"])
+    el = sg.EdgeList(path)
     csc = sg.CSCGraph()
     csc.createFromEdgeListFile(el.getNumVertices(), el.getNumEdges(), el.getSrcList(), el.getDstList())
-    return el, csc
+    return path, csc
 
 
-def reference_cpu(w, csc, n_colorings: int, threads: int, workdir: str):
-    """Runs the reference's own CLI (built from its sources) on graph.data; returns
-    (seconds per coloring, kind, note) or None."""
-    exe = os.path.join(ROOT, "oracle", "_ref", "sc-nec-ncc.bin")
-    n, edges = TEMPLATES[w["template"]]
+def write_template(workdir: str, n: int, edges) -> str:
     tpath = os.path.join(workdir, "template.fascia")
     with open(tpath, "w") as f:
         f.write(f"{n}\n{len(edges)}\n" + "".join(f"{a} {b}\n" for a, b in edges))
-    if os.path.exists(exe):
-        gpath = os.path.join(workdir, "graph.data")
-        csc.serialize(gpath)
-        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-        # argv: graph template iterations threads load_binary write_binary isPruned useSPMM
-        r = subprocess.run([exe, gpath, tpath, str(n_colorings), str(threads), "1", "0", "1", "1"],
-                           capture_output=True, text=True, env=env, cwd=workdir, timeout=1800)
-        m = re.search(r"Time for count per iter:\s*([0-9.eE+-]+)", r.stdout)
-        if r.returncode == 0 and m:
-            return float(m.group(1)), "reference", threads
-        log("reference CLI failed:", r.returncode, r.stderr[-500:])
-    # fall back to the oracle port (single thread) on one coloring
+    return tpath
+
+
+def reference_cli(gpath: str, n: int, edges, iters: int, threads: int, workdir: str):
+    """The reference's stock CLI (built from its sources, oracle/_ref/sc-nec-ncc.bin)
+    on a text edge list: argv graph template iterations threads load_binary=0
+    write_binary=0 isPruned=1 useSPMM=1.  Returns seconds per coloring (its
+    "Time for count per iter" line, which covers the counting loop only) or
+    None when the binary is missing or fails."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "sc-nec-ncc.bin")
+    if not os.path.exists(exe):
+        return None
+    tpath = write_template(workdir, n, edges)
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    r = subprocess.run([exe, gpath, tpath, str(iters), str(threads), "0", "0", "1", "1"],
+                       capture_output=True, text=True, env=env, cwd=workdir, timeout=3600)
+    m = re.search(r"Time for count per iter:\s*([0-9.eE+-]+)", r.stdout)
+    if r.returncode == 0 and m:
+        return float(m.group(1))
+    log("reference CLI failed:", r.returncode, r.stderr[-500:])
+    return None
+
+
+def reference_counts(gpath: str, n: int, edges, seed: int, ncol: int, threads: int, workdir: str):
+    """The reference's CountMat::colorCounting (oracle/_ref/ref_oracle, linked
+    from the reference's own objects) for colorings srand(seed) ..
+    srand(seed + ncol - 1) on the same text edge list: (raw counts, seconds of
+    each coloring), or None when the harness is missing."""
     from oracle import oracle as O
-    P = O.Plan(n, edges)
-    colors = O.colors(w["seed"], csc.getNumVertices(), n)
-    t0 = time.perf_counter()
-    O.count_coloring(csc.getIndexCol(), csc.getIndexRow(), P, colors)
-    return time.perf_counter() - t0, "port", 1
+    if not O.ref_available():
+        return None
+    tpath = write_template(workdir, n, edges)
+    R = O.run_ref(gpath, tpath, ncol, seed, os.path.join(workdir, "ref_out"), threads=threads, light=True)
+    return R["raw"], R["times"]
 
 
 def run_reference_arm(args, w):
+    """Rank 0 runs the reference's stock CLI: W warm-up colorings in one run, then
+    K timed colorings (one per step) in another; ms_per_step is its time per
+    coloring."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    _, csc = build_graph(w)
     threads = os.cpu_count() or 1
-    ncol = max(1, min(args.steps, 3))
+    n, edges = TEMPLATES[w["template"]]
+    gpath = graph_file(w["scale"], w["ef"])
     with tempfile.TemporaryDirectory() as tmp:
-        sec, kind, cores = reference_cpu(w, csc, ncol, threads, tmp)
+        if args.warmup > 0:
+            reference_cli(gpath, n, edges, args.warmup, threads, tmp)
+        sec = reference_cli(gpath, n, edges, args.steps, threads, tmp)
+    if sec is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/sc-nec-ncc.bin is missing or failed "
+                                                               "(build it with oracle/build_ref.sh)"}), flush=True)
+        return
     value = 1.0 / sec
     line = {
         "metric": METRIC, "value": value, "unit": "colorings/s", "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1000.0, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
         "config": config_of(args, w),
-        "cpu_baseline": {"value": value, "unit": "colorings/s", "cores": cores, "kind": kind,
-                         "sample": f"{ncol} coloring(s) of the workload, one process, {cores} threads"},
+        "step": "one coloring of the workload per step (the GPU arm's step is colorings_per_step colorings); "
+                "the metric is per coloring in both arms",
+        "cpu_baseline": {"value": value, "unit": "colorings/s", "cores": threads, "kind": "reference",
+                         "sample": f"{args.steps} colorings timed by the reference CLI's own counter after a "
+                                   f"{args.warmup}-coloring warm-up run, {threads} OpenMP threads, text edge "
+                                   f"list input"},
         "e2e": {"value": value, "unit": "colorings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -233,27 +272,26 @@ def run_mixed(args):
            "form": ("persistent job queue per graph" if args.persistent
                     else f"job streams per graph ({args.batch or 8} CUDA streams)"), "tables": "fp32", "sums": "fp64",
            "l2": "inputs larger than L2 at scales 18 and 20"}
-    graphs = []
-    for sc in MIXED["scales"]:
-        el = sg.rmat(sc, MIXED["ef"], seed=1)
-        csc = sg.CSCGraph()
-        csc.createFromEdgeListFile(el.getNumVertices(), el.getNumEdges(), el.getSrcList(), el.getDstList())
-        graphs.append(csc)
+    paths = [graph_file(sc, MIXED["ef"]) for sc in MIXED["scales"]]
     if args.impl == "reference":
         if rank != 0:
             return
         # the reference CLI on a bounded sample: the first jobs of the stream, one coloring each
         t_tot, done = 0.0, 0
+        cores = os.cpu_count() or 1
         with tempfile.TemporaryDirectory() as tmp:
             for gi, n, edges, seed in jobs:
                 if t_tot > 20.0 or done >= 32:
                     break
-                w = dict(template=f"job{done}", seed=seed)
-                TEMPLATES[w["template"]] = (n, edges)
-                sec, kind, cores = reference_cpu(w, graphs[gi], 1, os.cpu_count() or 1, tmp)
+                sec = reference_cli(paths[gi], n, edges, 1, cores, tmp)
+                if sec is None:
+                    print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/sc-nec-ncc.bin is missing "
+                                                                           "or failed"}), flush=True)
+                    return
                 t_tot += sec
                 done += 1
         value = done / t_tot
+        kind = "reference"
         print(json.dumps({"metric": METRIC, "value": value, "unit": "colorings/s", "impl": "reference",
                           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                           "ms_per_step": MIXED["jobs"] / value * 1000.0, "higher_is_better": True, "scaling": "weak",
@@ -265,6 +303,12 @@ def run_mixed(args):
         return
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    graphs = []
+    for path in paths:
+        el = sg.EdgeList(path)
+        csc = sg.CSCGraph()
+        csc.createFromEdgeListFile(el.getNumVertices(), el.getNumEdges(), el.getSrcList(), el.getDstList())
+        graphs.append(csc)
     dgs = [csc.device_graph(local) for csc in graphs]
     tmpls = [sg.Graph(n, e) for _, n, e, _ in jobs]
     by_graph = [[j for j, job in enumerate(jobs) if job[0] == gi] for gi in range(len(graphs))]
@@ -388,7 +432,7 @@ def main():
         return float(t.item())
 
     t_build = time.perf_counter()
-    el, csc = build_graph(w)
+    gpath, csc = build_graph(w)
     g = csc.device_graph(local)
     n, edges = TEMPLATES[w["template"]]
     tmpl = sg.Graph(n, edges)
@@ -398,8 +442,17 @@ def main():
     def seeds(step):  # rank-disjoint colorings
         return w["seed"] + (step * world + rank) * B
 
+    # warm-up; the first call on a new graph also times the tile-shape
+    # candidates of every stage shape (the autotuner): its wall time against
+    # the second call's is the tuning cost
+    warm_ms = []
     for s in range(args.warmup):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         sg.count(g, tmpl, B, seeds(s), batch=args.batch, hub_threshold=args.hub, persistent=args.persistent)
+        warm_ms.append((time.perf_counter() - t0) * 1000.0)
+    first_ms = warm_ms[0] if warm_ms else None
+    steady_ms = warm_ms[1] if len(warm_ms) > 1 else None
     barrier()
     dev_ms, launches, fused_ms, fused_launches, fused_bytes, gather_bytes, hub_ms = 0.0, 0, 0.0, 0, 0.0, 0.0, 0.0
     top = {"ms": 0.0, "bytes": 0.0, "launches": 0, "sub": -1}
@@ -497,16 +550,46 @@ def main():
                      "hub_ms_per_step": hub_ms / args.steps},
         "gpu_launches": launches,
         "clocks": clocks,
+        "autotune": {"first_call_ms": first_ms, "second_call_ms": steady_ms,
+                     "note": "wall clock of the first two warm-up steps: the first call on a new graph times "
+                             "the tile-shape candidates of each stage shape; later calls (the timed steps and "
+                             "the e2e leg, whose per-step graphs have the same signature) reuse the choice"},
     }
     if forms:
         line["forms"] = forms
     if e2e:
         line["e2e"] = e2e
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the reference's CountMat on the first two colorings this run timed, same
+        # graph file: its time is the CPU baseline, its raw counts the parity check
+        cores = os.cpu_count() or 1
+        s0 = seeds(args.warmup)
+        n_ref = min(2, B)
         with tempfile.TemporaryDirectory() as tmp:
-            sec, kind, cores = reference_cpu(w, csc, 1, os.cpu_count() or 1, tmp)
-        line["cpu_baseline"] = {"value": 1.0 / sec, "unit": "colorings/s", "cores": cores, "kind": kind,
-                                "sample": "1 coloring of the workload"}
+            got = reference_counts(gpath, n, edges, s0, n_ref, cores, tmp)
+        if got is not None:
+            ref_raw, ref_t = got
+            per = [abs(a - b) / abs(b) if b else abs(a - b) for a, b in zip(raws[0][:n_ref], ref_raw)]
+            est_gpu = sg.estimate(raws[0][:n_ref], n)
+            est_ref = sg.estimate(ref_raw, n)
+            line["rel_err_vs_reference"] = {
+                "per_coloring": per, "max": max(per), "estimate": abs(est_gpu - est_ref) / abs(est_ref) if est_ref else 0.0,
+                "seeds": [s0 + i for i in range(n_ref)],
+                "reference": "CountMat::colorCounting of the compiled reference (oracle/_ref/ref_oracle), same text "
+                             "edge list and seeds"}
+            line["cpu_baseline"] = {"value": 1.0 / float(ref_t.mean()), "unit": "colorings/s", "cores": cores,
+                                    "kind": "reference",
+                                    "sample": f"{n_ref} colorings (seeds {s0}..{s0 + n_ref - 1}) of the workload, "
+                                              f"counting loops on {cores} OpenMP threads"}
+        else:
+            # the oracle port on one coloring (single thread)
+            from oracle import oracle as O
+            P = O.Plan(n, edges)
+            colors = O.colors(s0, csc.getNumVertices(), n)
+            t0 = time.perf_counter()
+            O.count_coloring(csc.getIndexCol(), csc.getIndexRow(), P, colors)
+            line["cpu_baseline"] = {"value": 1.0 / (time.perf_counter() - t0), "unit": "colorings/s", "cores": 1,
+                                    "kind": "port", "sample": "1 coloring of the workload"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

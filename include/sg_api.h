@@ -41,7 +41,18 @@ typedef struct sg_countmat_s *sg_countmat;
 /* count modes */
 #define SG_MODE_REFERENCE 0   /* FP32 tables, the reference's arithmetic (isPruned=1) */
 #define SG_MODE_FP64 1        /* FP64 tables, no scaling: high-precision oracle mode */
-#define SG_MODE_ORIGINAL 2    /* FP32, isPruned=0 arithmetic (CountMat.cpp:851-977) */
+/* isPruned=0 (CountMat::countNonBottomeOriginal, CountMat.cpp:851-977): FP32,
+ * no 1e-12 scaling, FP32 root buffer, one SpMV per (output, split) pair.  On
+ * the reference's CSC graph the SpMV adds onto CountMat::_bufVec, which is
+ * zeroed only at initialization, so the aggregate accumulates over every
+ * split, sub-template and coloring of the run (CountMat.cpp:52-59, 931;
+ * CSCGraph.hpp:219-239): SG_MODE_ORIGINAL reproduces that, each sg_count
+ * call starting from a zero buffer (a fresh CountMat) and running its
+ * colorings one after another whatever `batch` says.  On a CSRGraph the SpMV
+ * overwrites its output (CSRGraph::SpMVNaiveFull, CSRGraph.cpp:190-208):
+ * SG_MODE_ORIGINAL_CSR, a fresh aggregation for every split. */
+#define SG_MODE_ORIGINAL 2
+#define SG_MODE_ORIGINAL_CSR 3
 
 const char *sg_last_error(void);
 const char *sg_version(void);
@@ -69,6 +80,15 @@ sg_status sg_graph_data_write(const char *path, int32_t V, int32_t numEdges, con
                               const int32_t *indexRow, const int32_t *degList);
 sg_status sg_graph_data_read(const char *path, int32_t *V, int32_t *numEdges, int32_t **indexCol,
                              int32_t **indexRow, int32_t **degList);
+/* The same bytes in memory, for callers that hold the stream or descriptor
+ * themselves (CSCGraph::serialize(ofstream&), deserialize(int fd),
+ * CSCGraph.hpp:71-72; CSRGraph::serialize/deserialize, CSRGraph.cpp:236-295,
+ * whose layout is the same with row offsets and column ids): *buf is
+ * malloc'd (release with sg_free). */
+sg_status sg_graph_data_encode(int32_t V, int32_t numEdges, const int32_t *offsets, const int32_t *neighbors,
+                               const int32_t *degList, void **buf, int64_t *bytes);
+sg_status sg_graph_data_decode(const void *buf, int64_t bytes, int32_t *V, int32_t *numEdges, int32_t **offsets,
+                               int32_t **neighbors, int32_t **degList);
 
 /* Synthetic input: seeded R-MAT (no reference counterpart in the product; the
  * reference's inputs come from graph500's make_graph, make_graph.h:21-35). */
@@ -146,9 +166,6 @@ typedef struct {
                                rounding) and hub neighbour lists summed in chunks */
     int32_t wait_limit_ms;  /* batched form: how long a work item may wait for its inputs
                                before the call fails with SG_ERR_TIMEOUT (0 = 2000 ms) */
-    int32_t test_unsatisfiable_wait; /* test hook: in the batched form the first fused stage
-                               also waits on a counter nothing increments, so the call
-                               must end with SG_ERR_TIMEOUT */
     int32_t no_blocked;     /* 1: no register-blocked eMA (every output computed by its
                                own split loop); the two forms give identical values */
     int32_t persistent;     /* batched form: 1 = one persistent work-queue launch per batch
@@ -215,10 +232,16 @@ sg_status sg_debug_sub_table(sg_graph g, sg_plan p, uint32_t seed, int32_t mode,
 /* per-vertex root values (bufLastSub, CountMat.cpp:815-831) and their sum */
 sg_status sg_debug_root(sg_graph g, sg_plan p, uint32_t seed, int32_t mode, int32_t hub_threshold,
                         double *root, double *raw);
+/* Test of the bounded waits (no counterpart in the reference): sg_count in the
+ * persistent batched form (opts->batch colorings per batch) with one extra
+ * dependency of the first fused stage on a counter that nothing increments,
+ * so the call must end with SG_ERR_TIMEOUT after opts->wait_limit_ms and
+ * leave the device usable.  Only for tests; sg_count has no such option. */
+sg_status sg_debug_count_unsatisfiable_wait(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw);
 
 /* The coloring of sg_colors for callers that cannot allocate device memory
  * (no counterpart in the reference).  Frameworks that reserve all GPU memory
- * in their own pool, and pipelines that cannot afford the device
+ * in their own pool at start-up, and pipelines that cannot take the device
  * synchronisation an allocation implies, pass the output buffer themselves:
  * d_colors is a DEVICE array of V int32 written with rand() % k after
  * srand(seed), in vertex order, on `stream` (a cudaStream_t; NULL = legacy
@@ -226,10 +249,13 @@ sg_status sg_debug_root(sg_graph g, sg_plan p, uint32_t seed, int32_t mode, int3
  * jump-ahead tables, 8.3 MB) is a fixed array in the library that every GPU
  * that loads the library keeps until the process exits; V is limited to 2^26
  * and larger V is rejected with SG_ERR_INVALID.  The first call on a device
- * looks up that array's address on the device and should come before any
- * stream capture.  Every call rewrites the tables it reads and waits for
- * that upload; calls that overlap on the GPU (other threads, other streams)
- * share the array and race. */
+ * is its set-up: it looks up the array's device address and fills the whole
+ * array with one synchronous copy from host memory, so that first call must
+ * not be made while a stream is being captured.  Every later call only
+ * launches one kernel on `stream` (no copy, no synchronisation).  All calls
+ * share the array; after the set-up they only read it, so calls that overlap
+ * on the GPU do not disturb one another, and concurrent first calls from
+ * several host threads are serialised by a lock. */
 sg_status sg_colors_noalloc(int32_t V, int32_t k, uint32_t seed, int32_t *d_colors, void *stream);
 
 /* ---- CountMat mirror ---------------------------------------------------- */

@@ -8,8 +8,10 @@
 # the one harness-side fix is applied there: Graph::operator= has no
 # `return *this;` (Graph.cpp:131-142), which GCC 13 turns into a trap.
 # Usage: oracle/build_ref.sh [REFERENCE_DIR]
+#   REFERENCE_DIR defaults to $SUBGRAPH_REFERENCE_DIR, else /root/reference.
+#   Exit status 2: the reference sources are not there (nothing is built).
 set -euo pipefail
-REF="${1:-/root/reference}"
+REF="${1:-${SUBGRAPH_REFERENCE_DIR:-/root/reference}}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 OUT="$HERE/_ref"
 SRC="$OUT/src"

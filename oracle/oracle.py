@@ -54,6 +54,8 @@ def lib():
         L.orc_plan_tables.argtypes = [vp, ctypes.c_int, vp, vp, vp]
         L.orc_count_coloring.argtypes = [vp, vp, i32, vp, vp, ctypes.c_int, vp]
         L.orc_count_coloring.restype = ctypes.c_double
+        L.orc_count_coloring_state.argtypes = [vp, vp, i32, vp, vp, ctypes.c_int, vp, vp]
+        L.orc_count_coloring_state.restype = ctypes.c_double
         L.orc_sub_table.argtypes = [vp, vp, i32, vp, vp, ctypes.c_int, vp]
         L.orc_sub_table.restype = ctypes.c_int
         L.orc_estimate.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
@@ -137,19 +139,32 @@ class Plan:
 
 MODE_REF = 0       # FP32 tables, reference arithmetic (isPruned=1)
 MODE_FP64 = 1      # FP64 tables, no scaling
-MODE_ORIGINAL = 2  # isPruned=0 arithmetic
+MODE_ORIGINAL = 2  # isPruned=0 on a CSC graph: the SpMV buffer accumulates (state carried)
+MODE_ORIGINAL_CSR = 3  # isPruned=0 on a CSR graph: a fresh aggregation per split
 
 
 def count_coloring(col: np.ndarray, row: np.ndarray, plan: Plan, color: np.ndarray,
-                   mode: int = MODE_REF, want_root: bool = False):
+                   mode: int = MODE_REF, want_root: bool = False, state: np.ndarray | None = None):
+    """One coloring's raw count.  Mode 2 starts from `state` (float32 [V], the
+    CountMat's SpMV buffer, updated in place) or from zeros."""
     V = len(col) - 1
     col = np.ascontiguousarray(col, np.int32)
     row = np.ascontiguousarray(row, np.int32)
     color = np.ascontiguousarray(color, np.int32)
     root = np.zeros(V, np.float64) if want_root else None
-    r = lib().orc_count_coloring(_p(col), _p(row), V, plan._h, _p(color), mode,
-                                 _p(root) if want_root else None)
+    if state is not None:
+        assert state.dtype == np.float32 and state.flags.c_contiguous and len(state) == V
+    r = lib().orc_count_coloring_state(_p(col), _p(row), V, plan._h, _p(color), mode,
+                                       _p(state) if state is not None else None, _p(root) if want_root else None)
     return (r, root) if want_root else r
+
+
+def count_colorings(col: np.ndarray, row: np.ndarray, plan: Plan, colors, mode: int = MODE_REF) -> np.ndarray:
+    """Raw counts of several colorings run one after another on one CountMat
+    (mode 2 carries its SpMV buffer from each coloring to the next)."""
+    V = len(col) - 1
+    state = np.zeros(V, np.float32) if mode == MODE_ORIGINAL else None
+    return np.array([count_coloring(col, row, plan, c, mode, state=state) for c in colors])
 
 
 def sub_table(col, row, plan: Plan, color, s: int) -> np.ndarray:
@@ -177,10 +192,17 @@ def ref_available() -> bool:
 
 
 def run_ref(graph_txt: str, template: str, ncol: int, seed: int, outdir: str, threads: int = 4,
-            dump_tables: bool = False, automorphisms: bool = False) -> dict:
+            dump_tables: bool = False, automorphisms: bool = False, is_pruned: int = 1, use_spmm: int = 1,
+            csr: bool = False, light: bool = False) -> dict:
+    """Runs the compiled reference's CountMat (oracle/_ref/ref_oracle) and
+    loads what it wrote: colorings seeded srand(seed + c) on one thread, the
+    counting loops on `threads` threads, with the isPruned / useSPMM flags of
+    CountMat::initialization and a CSRGraph instead of the CSCGraph when
+    csr=True.  light=True writes only the raw counts and per-coloring times."""
     exe = os.path.join(REF_DIR, "ref_oracle")
     subprocess.check_call([exe, graph_txt, template, str(ncol), str(seed), str(threads), outdir,
-                           "1" if dump_tables else "0", "1" if automorphisms else "0"],
+                           "1" if dump_tables else "0", "1" if automorphisms else "0", str(is_pruned),
+                           str(use_spmm), "1" if csr else "0", "1" if light else "0"],
                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
                           env=dict(os.environ, OMP_NUM_THREADS="1"))
     return load_ref_dump(outdir)
@@ -188,11 +210,23 @@ def run_ref(graph_txt: str, template: str, ncol: int, seed: int, outdir: str, th
 
 def load_ref_dump(d: str) -> dict:
     out: dict = {}
-    col = np.fromfile(os.path.join(d, "csc_col.i32"), np.int32)
-    out["col"] = col
-    out["row"] = np.fromfile(os.path.join(d, "csc_row.i32"), np.int32)
     out["raw"] = np.array([float(x) for x in open(os.path.join(d, "raw.txt")).read().split()])
-    V = len(col) - 1
+    tp = os.path.join(d, "times.txt")
+    if os.path.exists(tp):
+        out["times"] = np.array([float(x) for x in open(tp).read().split()])
+    out["aut"] = int(open(os.path.join(d, "aut.txt")).read())
+    pre = "csc" if os.path.exists(os.path.join(d, "csc_col.i32")) else "csr"
+    if not os.path.exists(os.path.join(d, f"{pre}_col.i32")):
+        return out   # light run
+    if pre == "csc":
+        col = np.fromfile(os.path.join(d, "csc_col.i32"), np.int32)
+        out["col"] = col
+        out["row"] = np.fromfile(os.path.join(d, "csc_row.i32"), np.int32)
+        V = len(col) - 1
+    else:
+        out["csr_row"] = np.fromfile(os.path.join(d, "csr_row.i32"), np.int32)
+        out["csr_col"] = np.fromfile(os.path.join(d, "csr_col.i32"), np.int32)
+        V = len(out["csr_row"]) - 1
     out["V"] = V
     c = np.fromfile(os.path.join(d, "colors.i32"), np.int32)
     out["colors"] = c.reshape(-1, V) if V else c
@@ -225,5 +259,4 @@ def load_ref_dump(d: str) -> dict:
     rd = os.path.join(d, "raw_dump.txt")
     if os.path.exists(rd):
         out["raw_dump"] = float(open(rd).read())
-    out["aut"] = int(open(os.path.join(d, "aut.txt")).read())
     return out

@@ -13,10 +13,22 @@
 // num_threads(thd_num) explicitly).
 //
 // Usage: ref_oracle <graph.txt> <template> <ncolorings> <seed_base> <threads>
-//                   <outdir> [dump_tables] [automorphisms]
-// Writes: outdir/csc_col.i32, csc_row.i32, plan.txt, colors.i32 (ncol x V),
-//         raw.txt (one %.17g per coloring), tables/s<k>.f32 (coloring 0,
-//         column-major [L][V], only when dump_tables=1), aut.txt.
+//                   <outdir> [dump_tables] [automorphisms] [isPruned] [useSPMM]
+//                   [csr] [light]
+//   isPruned, useSPMM: CountMat::initialization's flags (default 1, 1), which
+//     select countNonBottomePrunedSPMM / countNonBottomePruned /
+//     countNonBottomeOriginal (CountMat.cpp:291-302);
+//   csr=1: the graph is a CSRGraph (CSRGraph::createFromEdgeListFile) instead
+//     of a CSCGraph;
+//   light=1: only raw.txt, times.txt and aut.txt are written (large graphs).
+// Writes: outdir/csc_col.i32, csc_row.i32 (or csr_row.i32, csr_col.i32 for
+//         csr=1), plan.txt, colors.i32 (ncol x V), raw.txt (one %.17g per
+//         coloring), times.txt (seconds of each coloring), tables/s<k>.f32
+//         (coloring 0, column-major [L][V], only when dump_tables=1), aut.txt.
+// Colorings run in order 0..ncol-1 on one CountMat, as compute() runs them
+// (isPruned=0 on a CSC graph carries CountMat::_bufVec from one SpMV to the
+// next, across colorings, CountMat.cpp:931); with dump_tables=1 coloring 0 is
+// the dumped one.
 #include <vector>
 #include <algorithm>
 #include <string>
@@ -32,6 +44,7 @@
 #define private public
 #include "CountMat.hpp"
 #include "EdgeList.hpp"
+#include "CSRGraph.hpp"
 #undef private
 
 static long g_time_base = 0;
@@ -67,8 +80,10 @@ static double counting_with_dump(CountMat &cm, const std::string &dir)
         int *idxCombToCount = (cm.indexer.getSubCToCount())[s];
         if (subSize == 1)
             cm._dTable.countCurBottom(idxCombToCount, cm._colors_local);
+        else if (cm._isPruned == 1)
+            countTotal = cm._useSPMM == 1 ? cm.countNonBottomePrunedSPMM(s) : cm.countNonBottomePruned(s);
         else
-            countTotal = cm.countNonBottomePrunedSPMM(s);
+            countTotal = cm.countNonBottomeOriginal(s);
         if (s > 0 && (subSize > 1 || s == cm._total_sub_num - 1)) {
             int L = cm._dTable.getTableLen(s);
             std::vector<float> buf((size_t)L * V);
@@ -94,24 +109,44 @@ int main(int argc, char **argv)
     int thds = atoi(argv[5]);
     int dump_tables = argc > 7 ? atoi(argv[7]) : 0;
     int want_aut = argc > 8 ? atoi(argv[8]) : 0;
+    int is_pruned = argc > 9 ? atoi(argv[9]) : 1;
+    int use_spmm = argc > 10 ? atoi(argv[10]) : 1;
+    int use_csr = argc > 11 ? atoi(argv[11]) : 0;
+    int light = argc > 12 ? atoi(argv[12]) : 0;
     mkdir(dir.c_str(), 0755);
     mkdir((dir + "/tables").c_str(), 0755);
 
     EdgeList elist(graph);
     CSCGraph<int32_t, float> csc;
-    csc.createFromEdgeListFile(elist.getNumVertices(), elist.getNumEdges(), elist.getSrcList(), elist.getDstList(), false);
-    csc.splitCSC(4 * thds);
-    int V = csc.getNumVertices();
-    int nnz = csc.getNNZ();
-    write_bin(dir + "/csc_col.i32", csc.getIndexCol(), sizeof(int32_t) * (V + 1));
-    write_bin(dir + "/csc_row.i32", csc.getIndexRow(), sizeof(int32_t) * (size_t)nnz);
+    CSRGraph csr;
+    int V = 0, nnz = 0;
+    if (use_csr) {
+        csr.createFromEdgeListFile(elist.getNumVertices(), elist.getNumEdges(), elist.getSrcList(), elist.getDstList(),
+                                   false, false, false);
+        V = csr.getNumVertices();
+        nnz = csr.getNNZ();
+        if (!light) {
+            write_bin(dir + "/csr_row.i32", csr.getIndexRow(), sizeof(int32_t) * (V + 1));
+            write_bin(dir + "/csr_col.i32", csr.getIndexCol(), sizeof(int32_t) * (size_t)nnz);
+        }
+    } else {
+        csc.createFromEdgeListFile(elist.getNumVertices(), elist.getNumEdges(), elist.getSrcList(), elist.getDstList(),
+                                   false);
+        csc.splitCSC(4 * thds);
+        V = csc.getNumVertices();
+        nnz = csc.getNNZ();
+        if (!light) {
+            write_bin(dir + "/csc_col.i32", csc.getIndexCol(), sizeof(int32_t) * (V + 1));
+            write_bin(dir + "/csc_row.i32", csc.getIndexRow(), sizeof(int32_t) * (size_t)nnz);
+        }
+    }
 
     Graph input_template;
     input_template.read_enlist(tmpl);
 
     omp_set_num_threads(1);
     CountMat cm;
-    cm.initialization(nullptr, &csc, thds, ncol, 1, 1, -1, false);
+    cm.initialization(use_csr ? &csr : nullptr, use_csr ? nullptr : &csc, thds, ncol, is_pruned, use_spmm, -1, false);
 
     // CountMat::compute setup (CountMat.cpp:82-125, 174-197)
     cm._templates = &input_template;
@@ -123,12 +158,18 @@ int main(int argc, char **argv)
     cm.indexer.initialization(cm._color_num, cm._total_sub_num, &cm._subtmp_array, &cm.div_tp);
     cm._dTable.initDataTable(cm._subtmp_array, &cm.indexer, cm._total_sub_num, cm._color_num, V, thds, 1, cm._bufMatCols);
     int k = cm._color_num;
+    // as CountMat::compute allocates it (CountMat.cpp:174-197), so that the
+    // destructor's frees match
     cm._bufVecLeaf = (float **)malloc(k * sizeof(float *));
-    cm._bufVecLeaf[0] = (float *)aligned_alloc(64, ((size_t)V * k * sizeof(float) + 63) / 64 * 64);
-    for (int i = 1; i < k; ++i) cm._bufVecLeaf[i] = cm._bufVecLeaf[0] + (size_t)i * V;
+    if (use_spmm == 0) {
+        for (int i = 0; i < k; ++i) cm._bufVecLeaf[i] = (float *)aligned_alloc(64, ((size_t)V * sizeof(float) + 63) / 64 * 64);
+    } else {
+        cm._bufVecLeaf[0] = (float *)aligned_alloc(64, ((size_t)V * k * sizeof(float) + 63) / 64 * 64);
+        for (int i = 1; i < k; ++i) cm._bufVecLeaf[i] = cm._bufVecLeaf[0] + (size_t)i * V;
+    }
 
     // plan: one line per sub, then its tables
-    {
+    if (!light) {
         FILE *f = fopen((dir + "/plan.txt").c_str(), "w");
         int n = cm._total_sub_num;
         fprintf(f, "k %d nsub %d V %d nnz %d\n", k, n, V, nnz);
@@ -157,24 +198,31 @@ int main(int argc, char **argv)
         fclose(f);
     }
 
-    std::vector<int32_t> colors((size_t)ncol * V);
+    std::vector<int32_t> colors(light ? 0 : (size_t)ncol * V);
     FILE *fr = fopen((dir + "/raw.txt").c_str(), "w");
+    FILE *ft = fopen((dir + "/times.txt").c_str(), "w");
     for (int c = 0; c < ncol; ++c) {
         g_time_base = seed + c;
-        double raw = cm.colorCounting();  // the reference's own per-coloring function
-        std::memcpy(&colors[(size_t)c * V], cm._colors_local, sizeof(int32_t) * V);
+        const double t0 = omp_get_wtime();
+        double raw;
+        if (c == 0 && dump_tables) {
+            raw = counting_with_dump(cm, dir);
+            FILE *f = fopen((dir + "/raw_dump.txt").c_str(), "w");
+            fprintf(f, "%.17g\n", raw);
+            fclose(f);
+        } else {
+            raw = cm.colorCounting();  // the reference's own per-coloring function
+        }
+        const double t1 = omp_get_wtime();
+        if (!light) std::memcpy(&colors[(size_t)c * V], cm._colors_local, sizeof(int32_t) * V);
         fprintf(fr, "%.17g\n", raw);
+        fprintf(ft, "%.9f\n", t1 - t0);
+        fflush(fr);
+        fflush(ft);
     }
     fclose(fr);
-    write_bin(dir + "/colors.i32", colors.data(), colors.size() * sizeof(int32_t));
-
-    if (dump_tables) {
-        g_time_base = seed;
-        double raw0 = counting_with_dump(cm, dir);
-        FILE *f = fopen((dir + "/raw_dump.txt").c_str(), "w");
-        fprintf(f, "%.17g\n", raw0);
-        fclose(f);
-    }
+    fclose(ft);
+    if (!light) write_bin(dir + "/colors.i32", colors.data(), colors.size() * sizeof(int32_t));
     {
         FILE *f = fopen((dir + "/aut.txt").c_str(), "w");
         fprintf(f, "%d\n", want_aut ? cm.automorphismNum() : 1);

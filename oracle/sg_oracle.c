@@ -442,14 +442,86 @@ void orc_plan_tables(const orc_plan *P, int s, int *c2c, int *msplit, int *aspli
 /*           root accumulated per vertex in double (CountMat.cpp:556-849,    */
 /*           DataTableColMajor.cpp:346-400).                                  */
 /*   mode 1: FP64 tables, no scaling (the high-precision oracle).             */
-/*   mode 2: isPruned=0 (CountMat.cpp:851-977): FP32, no scaling, FP32 root, */
-/*           the aggregation taken on a zeroed buffer for every split.       */
+/*   mode 2: isPruned=0 on a CSC graph (CountMat.cpp:851-977): FP32, no      */
+/*           scaling, FP32 root; for every output i (lex) and split j one     */
+/*           SpMV adds the aux column onto the buffer _bufVec, zeroed only at */
+/*           CountMat::initialization (CountMat.cpp:52-59, 931;               */
+/*           CSCGraph.hpp:219-239), then obj += bufVec * main                 */
+/*           (arrayWiseFMANaive, DataTableColMajor.cpp:502-510).  `state`     */
+/*           (V floats, optional) is that buffer, carried in and out.         */
+/*   mode 3: isPruned=0 on a CSRGraph: the same, but the SpMV overwrites its  */
+/*           output (CSRGraph::SpMVNaiveFull, CSRGraph.cpp:190-208): a fresh */
+/*           aggregation for every split.                                     */
 /* Tables are column-major [L][V] like DataTableColMajor.                     */
 /* root_out (optional) receives the per-vertex root value (double).           */
 /* ------------------------------------------------------------------------- */
+static double count_original_acc(const int32_t *indexCol, const int32_t *indexRow, int32_t V, const orc_plan *P,
+                                 const int32_t *color, float *buf, double *root_out)
+{
+    int n = P->nsub, k = P->k, bottom = n - 1;
+    size_t Vs = (size_t)V;
+    float **tf = (float **)calloc((size_t)n, sizeof(float *));
+    double countSum = 0.0;
+    for (int s = n - 1; s >= 0; --s) {
+        int sz = P->size[s];
+        if (sz == 1) {
+            if (s == bottom) {
+                tf[s] = (float *)calloc((size_t)k * Vs, sizeof(float));
+                for (int32_t v = 0; v < V; ++v) tf[s][(size_t)P->c2c[s][color[v]] * Vs + v] = 1.0f;
+            }
+            continue;
+        }
+        int m = P->main_[s], a = P->aux_[s];
+        int mt = P->size[m] == 1 ? bottom : m;
+        int at = P->size[a] == 1 ? bottom : a;
+        int Ls = P->tlen[s], S = P->nsplit[s];
+        float *out = (float *)calloc(s > 0 ? (size_t)Ls * Vs : Vs, sizeof(float));
+        for (int i = 0; i < Ls; ++i) {
+            float *obj = s > 0 ? out + (size_t)P->c2c[s][i] * Vs : out;
+            for (int j = 0; j < S; ++j) {
+                const float *x = tf[at] + (size_t)P->asplit[s][i * S + j] * Vs;
+                const float *mm = tf[mt] + (size_t)P->msplit[s][i * S + j] * Vs;
+                for (int32_t v = 0; v < V; ++v) {
+                    float b = buf[v];
+                    for (int32_t e = indexCol[v]; e < indexCol[v + 1]; ++e) b = b + x[indexRow[e]];
+                    buf[v] = b;
+                    float prod = b * mm[v];
+                    obj[v] = obj[v] + prod;
+                }
+            }
+        }
+        if (s > 0) tf[s] = out;
+        else {
+            for (int32_t v = 0; v < V; ++v) countSum += out[v];
+            if (root_out) for (int32_t v = 0; v < V; ++v) root_out[v] = out[v];
+            free(out);
+        }
+        if (P->size[m] > 1) { free(tf[m]); tf[m] = NULL; }
+        if (P->size[a] > 1) { free(tf[a]); tf[a] = NULL; }
+    }
+    for (int s = 0; s < n; ++s) free(tf[s]);
+    free(tf);
+    return countSum;
+}
+
+double orc_count_coloring_state(const int32_t *indexCol, const int32_t *indexRow, int32_t V, const orc_plan *P,
+                                const int32_t *color, int mode, float *state, double *root_out);
+
 double orc_count_coloring(const int32_t *indexCol, const int32_t *indexRow, int32_t V,
                           const orc_plan *P, const int32_t *color, int mode, double *root_out)
 {
+    return orc_count_coloring_state(indexCol, indexRow, V, P, color, mode, NULL, root_out);
+}
+
+double orc_count_coloring_state(const int32_t *indexCol, const int32_t *indexRow, int32_t V, const orc_plan *P,
+                                const int32_t *color, int mode, float *state, double *root_out)
+{
+    if (mode == 2) {
+        float *buf = state ? state : (float *)calloc((size_t)V + 1, sizeof(float));
+        double r = count_original_acc(indexCol, indexRow, V, P, color, buf, root_out);
+        if (!state) free(buf);
+        return r;
+    }
     int n = P->nsub, k = P->k;
     int bottom = n - 1;
     size_t Vs = (size_t)V;

@@ -5,11 +5,12 @@ A drop-in for the counting path of dsc-nec/subgraph: the same inputs
 sub-template division and color-set indexing, and per-coloring counts from
 hand-written sm_100a kernels behind a C ABI (include/sg_api.h).
 """
-from .api import (DUMMY_VAL, MODE_FP64, MODE_ORIGINAL, MODE_REFERENCE, CountMat, CSCGraph, CSRGraph,
-                  DeviceGraph, DivideTemplates, EdgeList, Graph, IndexSys, SGError, count, count_jobs, debug_root,
+from .api import (DUMMY_VAL, MODE_FP64, MODE_ORIGINAL, MODE_ORIGINAL_CSR, MODE_REFERENCE, CountMat, CSCGraph, CSRGraph,
+                  DeviceGraph, DivideTemplates, EdgeList, Graph, IndexSys, SGError, count, count_jobs,
+                  debug_count_unsatisfiable_wait, debug_root,
                   debug_sub_table, estimate, rmat)
 from ._lib import LIB_PATH, lib
 
 __all__ = ["EdgeList", "CSCGraph", "CSRGraph", "DeviceGraph", "Graph", "DivideTemplates", "IndexSys", "CountMat",
-           "count", "count_jobs", "estimate", "rmat", "debug_sub_table", "debug_root", "MODE_REFERENCE", "MODE_FP64",
-           "MODE_ORIGINAL", "DUMMY_VAL", "SGError", "LIB_PATH", "lib"]
+           "count", "count_jobs", "estimate", "rmat", "debug_sub_table", "debug_root", "debug_count_unsatisfiable_wait", "MODE_REFERENCE", "MODE_FP64",
+           "MODE_ORIGINAL", "MODE_ORIGINAL_CSR", "DUMMY_VAL", "SGError", "LIB_PATH", "lib"]

@@ -22,18 +22,21 @@ SG_ERR_UNSUPPORTED = 6
 MODE_REFERENCE = 0
 MODE_FP64 = 1
 MODE_ORIGINAL = 2
+MODE_ORIGINAL_CSR = 3
 
 # every symbol include/sg_api.h declares
 EXPORTS = [
     "sg_last_error", "sg_version", "sg_free",
     "sg_edgelist_read", "sg_edgelist_write", "sg_csc_build", "sg_csr_build",
-    "sg_graph_data_write", "sg_graph_data_read", "sg_rmat_generate",
+    "sg_graph_data_write", "sg_graph_data_read", "sg_graph_data_encode", "sg_graph_data_decode",
+    "sg_rmat_generate",
     "sg_plan_create", "sg_plan_read", "sg_plan_destroy", "sg_plan_info", "sg_plan_sub",
     "sg_plan_tables", "sg_plan_automorphisms", "sg_plan_sub_edges",
     "sg_graph_create", "sg_graph_destroy", "sg_graph_info", "sg_graph_create_edges", "sg_graph_create_text",
     "sg_graph_create_rmat", "sg_graph_download_csc",
     "sg_count_opts_default", "sg_count", "sg_count_jobs", "sg_estimate",
-    "sg_colors", "sg_debug_sub_table", "sg_debug_root", "sg_colors_noalloc",
+    "sg_colors", "sg_debug_sub_table", "sg_debug_root", "sg_debug_count_unsatisfiable_wait",
+    "sg_colors_noalloc",
     "sg_countmat_create", "sg_countmat_destroy", "sg_countmat_initialization",
     "sg_countmat_set_seed", "sg_countmat_compute", "sg_countmat_raw",
 ]
@@ -49,7 +52,7 @@ class CountOpts(ctypes.Structure):
     _fields_ = [("n_colorings", ctypes.c_int32), ("seed_base", ctypes.c_uint32), ("mode", ctypes.c_int32),
                 ("batch", ctypes.c_int32), ("hub_threshold", ctypes.c_int32), ("profile", ctypes.c_int32),
                 ("no_autotune", ctypes.c_int32), ("exact", ctypes.c_int32), ("wait_limit_ms", ctypes.c_int32),
-                ("test_unsatisfiable_wait", ctypes.c_int32), ("no_blocked", ctypes.c_int32),
+                ("no_blocked", ctypes.c_int32),
                 ("persistent", ctypes.c_int32)]
 
 
@@ -85,6 +88,8 @@ def lib() -> ctypes.CDLL:
         "sg_csr_build": ([i32, i64, vp, vp, pp, pp, pp], i32),
         "sg_graph_data_write": ([ctypes.c_char_p, i32, i32, vp, vp, vp], i32),
         "sg_graph_data_read": ([ctypes.c_char_p, P(i32), P(i32), pp, pp, pp], i32),
+        "sg_graph_data_encode": ([i32, i32, vp, vp, vp, pp, P(i64)], i32),
+        "sg_graph_data_decode": ([vp, i64, P(i32), P(i32), pp, pp, pp], i32),
         "sg_rmat_generate": ([i32, i32, d, d, d, u64, P(i32), P(i64), pp, pp], i32),
         "sg_plan_create": ([i32, i32, vp, vp, pp], i32),
         "sg_plan_read": ([ctypes.c_char_p, pp], i32),
@@ -109,6 +114,7 @@ def lib() -> ctypes.CDLL:
         "sg_colors": ([vp, i32, u32, vp], i32),
         "sg_debug_sub_table": ([vp, vp, u32, i32, i32, i32, vp], i32),
         "sg_debug_root": ([vp, vp, u32, i32, i32, vp, P(d)], i32),
+        "sg_debug_count_unsatisfiable_wait": ([vp, vp, P(CountOpts), vp], i32),
         "sg_colors_noalloc": ([i32, i32, u32, vp, vp], i32),
         "sg_countmat_create": ([pp], i32),
         "sg_countmat_destroy": ([vp], None),

@@ -20,7 +20,7 @@ from typing import Iterable, Optional, Sequence
 
 import numpy as np
 
-from ._lib import (MODE_FP64, MODE_ORIGINAL, MODE_REFERENCE, CountOpts, CountStats, SGError, check, lib)
+from ._lib import (MODE_FP64, MODE_ORIGINAL, MODE_ORIGINAL_CSR, MODE_REFERENCE, CountOpts, CountStats, SGError, check, lib)
 
 DUMMY_VAL = 93620
 
@@ -441,8 +441,7 @@ class IndexSys:
 def count(graph: DeviceGraph, template: Graph, n_colorings: int = 1, seed_base: int = 0,
           mode: int = MODE_REFERENCE, batch: int = 0, hub_threshold: int = 1024,
           return_stats: bool = False, profile: bool = False, autotune: bool = True, exact: bool = False,
-          wait_limit_ms: int = 0, test_unsatisfiable_wait: bool = False, blocked: bool = True,
-          persistent: bool = False):
+          wait_limit_ms: int = 0, blocked: bool = True, persistent: bool = False):
     """Raw colorful counts of n_colorings colorings (coloring c uses srand(seed_base + c))."""
     o = CountOpts()
     lib().sg_count_opts_default(ctypes.byref(o))
@@ -455,7 +454,6 @@ def count(graph: DeviceGraph, template: Graph, n_colorings: int = 1, seed_base: 
     o.no_autotune = 0 if autotune else 1
     o.exact = 1 if exact else 0
     o.wait_limit_ms = wait_limit_ms
-    o.test_unsatisfiable_wait = 1 if test_unsatisfiable_wait else 0
     o.no_blocked = 0 if blocked else 1
     o.persistent = 1 if persistent else 0
     raw = np.zeros(n_colorings, np.float64)
@@ -463,6 +461,22 @@ def count(graph: DeviceGraph, template: Graph, n_colorings: int = 1, seed_base: 
     check(lib().sg_count(graph.handle, template.plan, ctypes.byref(o), _p(raw), ctypes.byref(st)))
     if return_stats:
         return raw, {k: getattr(st, k) for k, _ in CountStats._fields_}
+    return raw
+
+
+def debug_count_unsatisfiable_wait(graph: DeviceGraph, template: Graph, n_colorings: int, seed_base: int,
+                                   batch: int, wait_limit_ms: int):
+    """Test of the bounded waits: the persistent batched form with one dependency
+    that nothing satisfies.  Raises SGError (status 4, timeout) when the waits
+    give up as they must."""
+    o = CountOpts()
+    lib().sg_count_opts_default(ctypes.byref(o))
+    o.n_colorings = n_colorings
+    o.seed_base = seed_base & 0xFFFFFFFF
+    o.batch = batch
+    o.wait_limit_ms = wait_limit_ms
+    raw = np.zeros(n_colorings, np.float64)
+    check(lib().sg_debug_count_unsatisfiable_wait(graph.handle, template.plan, ctypes.byref(o), _p(raw)))
     return raw
 
 
@@ -572,4 +586,4 @@ class CountMat:
 
 __all__ = ["EdgeList", "CSCGraph", "CSRGraph", "DeviceGraph", "Graph", "DivideTemplates", "IndexSys", "CountMat",
            "count", "count_jobs", "estimate", "rmat", "debug_sub_table", "debug_root", "MODE_REFERENCE", "MODE_FP64",
-           "MODE_ORIGINAL", "DUMMY_VAL", "SGError"]
+           "MODE_ORIGINAL", "MODE_ORIGINAL_CSR", "DUMMY_VAL", "SGError"]

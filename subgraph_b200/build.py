@@ -88,7 +88,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if force or jobs or _stale(LIB, objs):
         _run(["nvcc", "-shared"] + ARCH + ["-o", LIB] + objs + ["-cudart", "static"])
     cli_src = os.path.join(CSRC, "sc_main.cpp")
-    if os.path.exists(cli_src) and (force or _stale(CLI, [cli_src, LIB] + deps)):
+    shim = [os.path.join(ROOT, "include", "subgraph_b200", f) for f in sorted(os.listdir(os.path.join(ROOT, "include", "subgraph_b200")))]
+    if os.path.exists(cli_src) and (force or _stale(CLI, [cli_src, LIB] + deps + shim)):
         _run([_cxx()] + CXX_FLAGS + ["-I" + os.path.join(ROOT, "include"), cli_src, "-o", CLI,
                                      "-L" + HERE, "-lsubgraph_b200", "-Wl,-rpath,$ORIGIN/.."])
     if verbose:

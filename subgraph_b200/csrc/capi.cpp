@@ -1,6 +1,7 @@
 // C ABI (include/sg_api.h) over the host planner and the device engine.
 #include "../../include/sg_api.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -27,7 +28,10 @@ struct sg_countmat_s {
     uint32_t seed = 0;
     bool seeded = false;
     bool initialized = false;
+    bool csr = false;                 // the graph was given as the CSRGraph
     std::vector<double> raw;
+    std::vector<float> orig_state;    // isPruned=0 on a CSC graph: CountMat::_bufVec, zeroed at
+                                      // initialization and carried from one compute() to the next
 };
 
 namespace {
@@ -156,6 +160,49 @@ sg_status sg_graph_data_read(const char *path, int32_t *V, int32_t *numEdges, in
     *numEdges = g.numEdges;
     *indexCol = dup_array(g.indexCol);
     *indexRow = dup_array(g.indexRow);
+    *degList = dup_array(g.degList);
+    return SG_OK;
+    SG_GUARD_END
+}
+
+sg_status sg_graph_data_encode(int32_t V, int32_t numEdges, const int32_t *offsets, const int32_t *neighbors,
+                               const int32_t *degList, void **buf, int64_t *bytes)
+{
+    SG_GUARD_BEGIN
+    if (V < 0 || !offsets || !degList || !buf || !bytes) return fail(SG_ERR_INVALID, "null argument");
+    sg::CSC g;
+    g.V = V;
+    g.numEdges = numEdges;
+    g.indexCol.assign(offsets, offsets + V + 1);
+    int32_t nnz = offsets[V];
+    if (nnz < 0 || (nnz > 0 && !neighbors)) return fail(SG_ERR_INVALID, "bad offsets");
+    g.indexRow.assign(neighbors, neighbors + nnz);
+    g.degList.assign(degList, degList + V);
+    std::string b;
+    sg::encode_graph_data(g, b);
+    void *p = std::malloc(std::max<size_t>(b.size(), 1));
+    if (!p) return fail(SG_ERR_OOM, "host allocation failed");
+    std::memcpy(p, b.data(), b.size());
+    *buf = p;
+    *bytes = (int64_t)b.size();
+    return SG_OK;
+    SG_GUARD_END
+}
+
+sg_status sg_graph_data_decode(const void *buf, int64_t bytes, int32_t *V, int32_t *numEdges, int32_t **offsets,
+                               int32_t **neighbors, int32_t **degList)
+{
+    SG_GUARD_BEGIN
+    if ((!buf && bytes > 0) || bytes < 0 || !V || !numEdges || !offsets || !neighbors || !degList)
+        return fail(SG_ERR_INVALID, "null argument");
+    sg::CSC g;
+    std::string err;
+    if (!sg::decode_graph_data((const char *)buf, (size_t)bytes, "graph.data buffer", g, err))
+        return fail(SG_ERR_INVALID, err);
+    *V = g.V;
+    *numEdges = g.numEdges;
+    *offsets = dup_array(g.indexCol);
+    *neighbors = dup_array(g.indexRow);
     *degList = dup_array(g.degList);
     return SG_OK;
     SG_GUARD_END
@@ -348,10 +395,9 @@ void sg_count_opts_default(sg_count_opts *o)
     o->hub_threshold = 1024;
 }
 
-sg_status sg_count(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw, sg_count_stats *stats)
+namespace {
+sg::CountOptions count_options(const sg_count_opts *o)
 {
-    SG_GUARD_BEGIN
-    if (!g || !p || !o || !raw) return fail(SG_ERR_INVALID, "null argument");
     sg::CountOptions co;
     co.n_colorings = o->n_colorings;
     co.seed_base = o->seed_base;
@@ -362,9 +408,17 @@ sg_status sg_count(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw, s
     co.autotune = o->no_autotune ? 0 : 1;
     co.exact = o->exact ? 1 : 0;
     co.wait_limit_ms = o->wait_limit_ms;
-    co.test_unsatisfiable_wait = o->test_unsatisfiable_wait;
     co.blocked = o->no_blocked ? 0 : 1;
     co.persistent = o->persistent;
+    return co;
+}
+}  // namespace
+
+sg_status sg_count(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw, sg_count_stats *stats)
+{
+    SG_GUARD_BEGIN
+    if (!g || !p || !o || !raw) return fail(SG_ERR_INVALID, "null argument");
+    sg::CountOptions co = count_options(o);
     sg::CountStats cs;
     sg_status st = from(sg::count(*g->g, p->p, co, raw, &cs));
     if (st) return st;
@@ -383,6 +437,18 @@ sg_status sg_count(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw, s
         stats->top_alg_bytes = cs.top_alg_bytes;
     }
     return SG_OK;
+    SG_GUARD_END
+}
+
+sg_status sg_debug_count_unsatisfiable_wait(sg_graph g, sg_plan p, const sg_count_opts *o, double *raw)
+{
+    SG_GUARD_BEGIN
+    if (!g || !p || !o || !raw) return fail(SG_ERR_INVALID, "null argument");
+    if (o->batch < 1) return fail(SG_ERR_INVALID, "the wait test runs the batched form: batch must be >= 1");
+    sg::CountOptions co = count_options(o);
+    co.persistent = 1;
+    co.test_unsatisfiable_wait = 1;
+    return from(sg::count(*g->g, p->p, co, raw, nullptr));
     SG_GUARD_END
 }
 
@@ -477,6 +543,8 @@ sg_status sg_countmat_initialization(sg_countmat cm, sg_graph csr_graph, sg_grap
         return fail(SG_ERR_INVALID, "exactly one of the CSR and CSC graphs must be given");
     if (itr_num < 1) return fail(SG_ERR_INVALID, "itr_num must be >= 1");
     cm->graph = csr_graph ? csr_graph : csc_graph;
+    cm->csr = csr_graph != nullptr;
+    cm->orig_state.assign((size_t)cm->graph->g->V, 0.0f);
     cm->thd_num = thd_num;
     cm->itr_num = itr_num;
     cm->isPruned = isPruned;
@@ -505,10 +573,16 @@ sg_status sg_countmat_compute(sg_countmat cm, sg_plan templates, int32_t isEstim
     sg_count_opts_default(&o);
     o.n_colorings = cm->itr_num;
     o.seed_base = cm->seeded ? cm->seed : (uint32_t)std::time(nullptr);
-    o.mode = cm->isPruned ? SG_MODE_REFERENCE : SG_MODE_ORIGINAL;
+    // isPruned=0 differs by graph type: the CSC path accumulates its SpMV buffer
+    // (CountMat.cpp:931, CSCGraph.hpp:219-239), the CSR path overwrites it
+    // (CSRGraph::SpMVNaiveFull, CSRGraph.cpp:190-208); useSPMM selects between
+    // aggregations with identical results (CountMat.cpp:325-554 vs 556-849)
+    o.mode = cm->isPruned ? SG_MODE_REFERENCE : (cm->csr ? SG_MODE_ORIGINAL_CSR : SG_MODE_ORIGINAL);
     cm->raw.assign((size_t)cm->itr_num, 0.0);
-    sg_count_stats stats;
-    sg_status st = sg_count(cm->graph, templates, &o, cm->raw.data(), &stats);
+    sg::CountOptions co = count_options(&o);
+    if (o.mode == SG_MODE_ORIGINAL) co.orig_state = cm->orig_state.data();
+    sg::CountStats stats;
+    sg_status st = from(sg::count(*cm->graph->g, templates->p, co, cm->raw.data(), &stats));
     if (st) return st;
     const int k = templates->p.k;
     if (verbose) {

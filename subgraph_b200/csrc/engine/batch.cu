@@ -123,27 +123,11 @@ __global__ void __launch_bounds__(kBatchThreads, 2)
 __global__ void k_root_reduce_slots(const double *__restrict__ partial, int64_t slot_stride, int32_t n,
                                     const int32_t *__restrict__ n_slot, double scale, double *out)
 {
-    __shared__ double ss[256], cc[256];
+    __shared__ double ss[256], cc[256], pp[256];
     const double *p = partial + (size_t)blockIdx.x * slot_stride;
     if (n_slot) n = n_slot[blockIdx.x];   // jobs of different templates: their own tile counts
-    double s = 0.0, c = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const double y = __dadd_rn(p[i], -c);
-        const double t = __dadd_rn(s, y);
-        c = __dadd_rn(__dadd_rn(t, -s), -y);
-        s = t;
-    }
-    ss[threadIdx.x] = s;
-    cc[threadIdx.x] = c;
-    __syncthreads();
-    for (int w = 128; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) {
-            ss[threadIdx.x] = __dadd_rn(ss[threadIdx.x], ss[threadIdx.x + w]);
-            cc[threadIdx.x] = __dadd_rn(cc[threadIdx.x], cc[threadIdx.x + w]);
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) out[blockIdx.x] = __dmul_rn(__dadd_rn(ss[0], -cc[0]), scale);
+    const double r = block_sum_partials(p, n, scale, ss, cc, pp);
+    if (threadIdx.x == 0) out[blockIdx.x] = r;
 }
 
 cudaError_t launch_persistent(const BatchStage *stages, int nstages, int total_items, int *done, BatchCtl *ctl,

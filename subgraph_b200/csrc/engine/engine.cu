@@ -103,11 +103,14 @@ struct Workspace {
     size_t root_vertex_bytes = 0;
     int32_t *adjc = nullptr;           // [nnz] neighbour id | color << 28 of the coloring in slot 0
     size_t adjc_bytes = 0;
+    float *orig_buf = nullptr;         // [V] isPruned=0 (CSC) aggregation buffer, internal order
+    size_t orig_buf_bytes = 0;
     uint64_t generation = 0;   // bumped whenever a buffer above is re-allocated
 };
 
 struct DevicePlanTables {
     std::vector<uint32_t *> split;   // per sub
+    std::vector<int32_t *> c2c;      // per sub: output column of each color set in lexicographic order
     std::vector<int16_t *> rem;      // per sub
     std::vector<uint32_t *> aoff, moff;  // per sub: packed-layout byte offsets (FP32)
     std::vector<int32_t *> blk;      // per sub: register-blocked eMA column tables, or null
@@ -361,6 +364,7 @@ Status upload_plan(DeviceGraph &g, const Plan &p, DevicePlanTables &out)
     out.blk_shape.assign(p.nsub(), 0);
     out.blk_nblocks.assign(p.nsub(), 0);
     out.split.assign(p.nsub(), nullptr);
+    out.c2c.assign(p.nsub(), nullptr);
     out.rem.assign(p.nsub(), nullptr);
     out.aoff.assign(p.nsub(), nullptr);
     out.moff.assign(p.nsub(), nullptr);
@@ -378,6 +382,9 @@ Status upload_plan(DeviceGraph &g, const Plan &p, DevicePlanTables &out)
         }
         SG_CK(cudaMallocAsync(&out.split[s], sp.size() * 4, g.stream));
         SG_CK(cudaMemcpyAsync(out.split[s], sp.data(), sp.size() * 4, cudaMemcpyHostToDevice, g.stream));
+        SG_CK(cudaMallocAsync(&out.c2c[s], (size_t)st.L * 4, g.stream));
+        SG_CK(cudaMemcpyAsync(out.c2c[s], st.comb_to_count.data(), (size_t)st.L * 4, cudaMemcpyHostToDevice, g.stream));
+        SG_CK(cudaStreamSynchronize(g.stream));   // `sp` is pageable and goes out of scope
         if (p.subs[st.main].size > 1 && s != 0) {
             // packed eMA: byte offsets of the aggregate row and of the main row
             // (main rows follow the La_rows aggregate rows) in the shared tile
@@ -453,10 +460,11 @@ DeviceGraph::~DeviceGraph()
         if (it != g_state.end()) {
             Workspace &w = it->second.ws;
             for (void *p : {w.arena, (void *)w.colors, (void *)w.partial, (void *)w.raw, (void *)w.windows, w.hub_partial,
-                            (void *)w.chunk_start, (void *)w.root_vertex, (void *)w.adjc})
+                            (void *)w.chunk_start, (void *)w.root_vertex, (void *)w.adjc, (void *)w.orig_buf})
                 if (p) cudaFreeAsync(p, stream);
             for (auto &kv : it->second.plans) {
                 for (auto *p : kv.second.split) if (p) cudaFreeAsync(p, stream);
+                for (auto *p : kv.second.c2c) if (p) cudaFreeAsync(p, stream);
                 for (auto *p : kv.second.rem) if (p) cudaFreeAsync(p, stream);
                 for (auto *p : kv.second.aoff) if (p) cudaFreeAsync(p, stream);
                 for (auto *p : kv.second.blk) if (p) cudaFreeAsync(p, stream);
@@ -677,6 +685,7 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
     SG_CKS(growT(&w.raw, &w.raw_bytes, 8 * (size_t)std::max(ncolorings_total, 1), g.stream));
     SG_CKS(growT(&w.windows, &w.windows_bytes, 4 * 31 * (size_t)std::max(ncolorings_total, 1), g.stream));
     if (c.use_adjc) SG_CKS(growT(&w.adjc, &w.adjc_bytes, std::max<size_t>(16, 4 * (size_t)g.nnz), g.stream));
+    if (c.mode == kModeOriginal) SG_CKS(growT(&w.orig_buf, &w.orig_buf_bytes, std::max<size_t>(16, 4 * V), g.stream));
     if (c.hubs.count > 0) {
         // a partial row holds the aux columns (or colour counts) of up to c.lay colorings
         int32_t maxp = round_up(c.lay * c.p.k, 8);
@@ -727,7 +736,7 @@ StageDesc make_stage(RunCtx &c, int slot, int s, double *root_vertex, int b0 = 0
     d.L_a = a.L;
     d.is_root = s == 0;
     d.scaled = (c.mode == kModeReference && s == p.scaled_sub && s != 0) ? 1 : 0;
-    d.root_float = c.mode == kModeOriginal;
+    d.root_float = c.mode == kModeOriginal || c.mode == kModeOriginalCSR;
     const int L = c.lay;
     const int ps = s == 0 ? 0 : p.table_pitch[s];
     const int pm = d.main_leaf ? 0 : p.table_pitch[sub.main];
@@ -798,9 +807,46 @@ HubArgs make_hub(RunCtx &c, StageDesc &d, void *partial)
     return h;
 }
 
+// One isPruned=0 step on a CSC graph (k_original): the running aggregation
+// buffer is the workspace's orig_buf.
+Status run_stage_original(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t st)
+{
+    const Plan &p = c.p;
+    const SubTemplate &sub = p.subs[s];
+    const SubTemplate &m = p.subs[sub.main], &a = p.subs[sub.aux];
+    OriginalArgs o{};
+    o.V = c.g.V;
+    o.L_s = sub.L;
+    o.S = sub.S;
+    o.split_stride = (sub.L + 3) / 4 * 4;
+    o.split = c.tab->split[s];
+    o.c2c = c.tab->c2c[s];
+    o.main_leaf = m.size == 1;
+    o.aux_leaf = a.size == 1;
+    o.is_root = s == 0;
+    o.main = o.main_leaf ? nullptr : (const float *)table_ptr(c, slot, sub.main);
+    o.main_pitch = o.main_leaf ? 0 : p.table_pitch[sub.main];
+    o.aux = o.aux_leaf ? nullptr : (const float *)table_ptr(c, slot, sub.aux);
+    o.aux_pitch = o.aux_leaf ? 0 : p.table_pitch[sub.aux];
+    o.out = s == 0 ? nullptr : (float *)table_ptr(c, slot, s);
+    o.out_pitch = s == 0 ? 0 : p.table_pitch[s];
+    o.color = c.gs.ws.colors + (size_t)slot * c.g.V;
+    o.off = c.g.d_off;
+    o.adj = c.g.d_adj;
+    o.buf = c.gs.ws.orig_buf;
+    o.partial = c.gs.ws.partial + (size_t)slot * (c.g.V / 8 + 2);
+    o.root_vertex = root_vertex;
+    const int blocks = launch_original(o, st);
+    c.launches += 1;
+    if (s == 0) c.root_tiles = blocks;
+    SG_CK(cudaGetLastError());
+    return Status::ok();
+}
+
 // One sub-template step of the coloring in color slot `slot`.
 Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t st, int b0 = 0, int nb = 1)
 {
+    if (c.mode == kModeOriginal) return run_stage_original(c, slot, s, root_vertex, st);
     DeviceGraph &g = c.g;
     StageDesc d = make_stage(c, slot, s, root_vertex, b0, nb);
     if (c.hubs.count > 0) {
@@ -1386,7 +1432,7 @@ Status count_grouped(RunCtx &c, const CountOptions &o, double *raw, CountStats *
 Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, CountStats *stats)
 {
     if (o.n_colorings < 1) return Status{1, "n_colorings must be >= 1"};
-    if (o.mode < 0 || o.mode > 2) return Status{1, "unknown count mode"};
+    if (o.mode < 0 || o.mode > 3) return Status{1, "unknown count mode"};
     if (p.k > 255) return Status{1, "too many colors"};
     if (g.V >= (1 << 28)) return Status{1, "counting supports graphs of fewer than 2^28 vertices"};
     SG_CK(cudaSetDevice(g.device));
@@ -1398,17 +1444,26 @@ Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, 
     c.profile = o.profile != 0;
     c.autotune = o.autotune != 0;
     c.blocked = o.blocked != 0;
-    if (o.batch > 0) return o.persistent ? count_batched(c, o, raw, stats) : count_grouped(c, o, raw, stats);
+    // mode 2 carries its aggregation buffer from one coloring to the next, so
+    // its colorings always run one after another (the plain form)
+    if (o.batch > 0 && o.mode != kModeOriginal)
+        return o.persistent ? count_batched(c, o, raw, stats) : count_grouped(c, o, raw, stats);
     const int slots = 1;
     c.use_adjc = adjc_ok(g, p);
     SG_CKS(prepare(c, slots, o.n_colorings));
     SG_CKS(upload_windows(c, o.seed_base, o.n_colorings));
     cudaStream_t st = g.stream;
+    if (o.mode == kModeOriginal) {
+        if (o.orig_state)
+            SG_CK(cudaMemcpyAsync(gs.ws.orig_buf, o.orig_state, 4 * (size_t)g.V, cudaMemcpyHostToDevice, st));
+        else
+            SG_CK(cudaMemsetAsync(gs.ws.orig_buf, 0, 4 * (size_t)g.V, st));
+    }
     cudaEvent_t e0, e1;
     SG_CK(cudaEventCreate(&e0));
     SG_CK(cudaEventCreate(&e1));
     SG_CK(cudaEventRecord(e0, st));
-    const double scale = o.mode == kModeOriginal ? 1.0 : (o.mode == kModeReference ? 1.0e12 : 1.0);
+    const double scale = o.mode == kModeReference ? 1.0e12 : 1.0;
     for (int col = 0; col < o.n_colorings; ++col) {
         SG_CKS(launch_colors(c, 0, col, 1, st));
         for (int s : p.process_order) SG_CKS(run_stage(c, 0, s, nullptr, st));
@@ -1418,6 +1473,8 @@ Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, 
     }
     SG_CK(cudaEventRecord(e1, st));
     SG_CK(cudaMemcpyAsync(raw, gs.ws.raw, sizeof(double) * o.n_colorings, cudaMemcpyDeviceToHost, st));
+    if (o.mode == kModeOriginal && o.orig_state)
+        SG_CK(cudaMemcpyAsync(o.orig_state, gs.ws.orig_buf, 4 * (size_t)g.V, cudaMemcpyDeviceToHost, st));
     SG_CK(cudaStreamSynchronize(st));
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
@@ -1474,6 +1531,7 @@ static Status run_partial(DeviceGraph &g, const Plan &p, uint32_t seed, int mode
     SG_CKS(prepare(c, 1, 1));
     SG_CKS(upload_windows(c, seed, 1));
     SG_CKS(launch_colors(c, 0, 0, 1, g.stream));
+    if (mode == kModeOriginal) SG_CK(cudaMemsetAsync(gs.ws.orig_buf, 0, 4 * (size_t)g.V, g.stream));
     for (int s : p.process_order) {
         if (s < upto) break;
         SG_CKS(run_stage(c, 0, s, upto == 0 ? gs.ws.root_vertex : nullptr, g.stream));
@@ -1556,6 +1614,10 @@ Status count_jobs_streams(DeviceGraph &g, const std::vector<const Plan *> &plans
 Status count_jobs(DeviceGraph &g, const std::vector<const Plan *> &plans, const uint32_t *seeds,
                   const CountOptions &o, double *raw, double *job_ms, CountStats *stats)
 {
+    if (o.mode == kModeOriginal)
+        return Status{6, "mode 2 (isPruned=0 on a CSC graph) carries its aggregation buffer from one coloring to the "
+                         "next: count such jobs with sg_count one after another"};
+    if (o.mode < 0 || o.mode > 3) return Status{1, "unknown count mode"};
     if (!o.persistent) return count_jobs_streams(g, plans, seeds, o, raw, job_ms, stats);
     const int n = (int)plans.size();
     if (n < 1) return Status{1, "no jobs"};

@@ -348,30 +348,80 @@ void launch_color_adj(const int32_t *adj, int64_t nnz, const uint8_t *color, int
 // ---------------------------------------------------------------------------
 __global__ void k_root_reduce(const double *__restrict__ partial, int32_t n, double scale, double *out)
 {
-    __shared__ double ss[256], cc[256];
-    double s = 0.0, c = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const double y = __dadd_rn(partial[i], -c);
-        const double t = __dadd_rn(s, y);
-        c = __dadd_rn(__dadd_rn(t, -s), -y);
-        s = t;
-    }
-    ss[threadIdx.x] = s;
-    cc[threadIdx.x] = c;
-    __syncthreads();
-    for (int w = 128; w > 0; w >>= 1) {
-        if ((int)threadIdx.x < w) {
-            ss[threadIdx.x] = __dadd_rn(ss[threadIdx.x], ss[threadIdx.x + w]);
-            cc[threadIdx.x] = __dadd_rn(cc[threadIdx.x], cc[threadIdx.x + w]);
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) *out = __dmul_rn(__dadd_rn(ss[0], -cc[0]), scale);
+    __shared__ double ss[256], cc[256], pp[256];
+    const double r = block_sum_partials(partial, n, scale, ss, cc, pp);
+    if (threadIdx.x == 0) *out = r;
 }
 
 void launch_root_reduce(const double *partial, int32_t n, double scale, double *out, cudaStream_t st)
 {
     k_root_reduce<<<1, 256, 0, st>>>(partial, n, scale, out);
+}
+
+// ---------------------------------------------------------------------------
+// isPruned=0 on a CSC graph (CountMat::countNonBottomeOriginal,
+// CountMat.cpp:851-977): for every output color set i in lexicographic order
+// and every split j in order, one SpMV adds the aux column auxSplit[i][j] of
+// every neighbour onto CountMat::_bufVec -- a buffer that is zeroed once, at
+// CountMat::initialization (CountMat.cpp:52-59), and never again, so it keeps
+// accumulating over splits, sub-templates and colorings (spmvNaiveSplit adds,
+// CSCGraph.hpp:219-239) -- and arrayWiseFMANaive adds bufVec * main to the
+// output column (DataTableColMajor.cpp:502-510); the root is an FP32 buffer.
+// Every vertex's bufVec entry is its own sequential chain of FP32 adds in
+// neighbour order, so one thread per vertex reproduces it exactly; the work
+// per vertex is degree x (sum over sub-templates of outputs x splits), as in
+// the reference.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kOriginalThreads) k_original(OriginalArgs a)
+{
+    __shared__ double red[kOriginalThreads / 32];
+    const int v = blockIdx.x * kOriginalThreads + threadIdx.x;
+    double rootv = 0.0;
+    if (v < a.V) {
+        float buf = a.buf[v];
+        const int cv = a.color[v];
+        const int beg = a.off[v], end = a.off[v + 1];
+        for (int i = 0; i < a.L_s; ++i) {
+            const int o = a.c2c[i];
+            float acc = 0.f;
+            for (int j = 0; j < a.S; ++j) {
+                const uint32_t pk = a.split[(size_t)j * a.split_stride + o];
+                const int mc = (int)(pk & 0xffffu), ac = (int)(pk >> 16);
+                for (int e = beg; e < end; ++e) {
+                    const int u = a.adj[e];
+                    const float x = a.aux_leaf ? (a.color[u] == ac ? 1.f : 0.f) : a.aux[(size_t)u * a.aux_pitch + ac];
+                    buf = __fadd_rn(buf, x);
+                }
+                const float m = a.main_leaf ? (cv == mc ? 1.f : 0.f) : a.main[(size_t)v * a.main_pitch + mc];
+                acc = __fadd_rn(acc, __fmul_rn(buf, m));
+            }
+            if (a.is_root) rootv = (double)acc;
+            else a.out[(size_t)v * a.out_pitch + o] = acc;
+        }
+        if (!a.is_root)
+            for (int o = a.L_s; o < a.out_pitch; ++o) a.out[(size_t)v * a.out_pitch + o] = 0.f;   // row padding
+        a.buf[v] = buf;
+        if (a.is_root && a.root_vertex) a.root_vertex[v] = rootv;
+    }
+    if (!a.is_root) return;
+    // the block's root values summed in a fixed order
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) rootv = __dadd_rn(rootv, __shfl_down_sync(0xffffffffu, rootv, o));
+    if (lane == 0) red[warp] = rootv;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < kOriginalThreads / 32; ++w) s = __dadd_rn(s, red[w]);
+        a.partial[blockIdx.x] = s;
+    }
+}
+
+int launch_original(const OriginalArgs &a, cudaStream_t st)
+{
+    const int blocks = (a.V + kOriginalThreads - 1) / kOriginalThreads;
+    if (blocks > 0) k_original<<<blocks, kOriginalThreads, 0, st>>>(a);
+    return blocks;
 }
 
 }  // namespace sg

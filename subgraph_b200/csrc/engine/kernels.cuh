@@ -67,6 +67,29 @@ void launch_hub(const HubArgs &h, bool fp64, int sm_count, cudaStream_t st);
 void launch_fused_blk(const StageDesc &d, const FusedConfig &cfg, cudaStream_t st);
 void launch_root_reduce(const double *partial, int32_t n, double scale, double *out, cudaStream_t st);
 
+// isPruned=0 on a CSC graph: one sub-template step, one thread per vertex,
+// with the running aggregation buffer carried in buf[V] (internal order)
+constexpr int kOriginalThreads = 256;
+struct OriginalArgs {
+    int32_t V, L_s, S, split_stride;
+    const uint32_t *split;     // [S][split_stride] main col | aux col << 16, per output column
+    const int32_t *c2c;        // [L_s] output column of the i-th color set in lexicographic order
+    int32_t main_leaf, aux_leaf, is_root;
+    const float *main;
+    int32_t main_pitch;
+    const float *aux;
+    int32_t aux_pitch;
+    float *out;
+    int32_t out_pitch;
+    const uint8_t *color;      // [V] internal order
+    const int32_t *off, *adj;
+    float *buf;                // [V] CountMat::_bufVec, internal order
+    double *partial;           // root: [blocks] per-block sums
+    double *root_vertex;       // root: [V] optional
+};
+// returns the number of blocks (= root partials written)
+int launch_original(const OriginalArgs &a, cudaStream_t st);
+
 // the batched form (batch.cu)
 // stage_end (optional): [nstages] %globaltimer when each stage's last item
 // completed, ctl->t0 when item 0 was claimed

@@ -111,62 +111,75 @@ sg_status fail(sg_status code, const std::string &msg)
     return code;
 }
 
+// Fills the whole scratch array for the current device: the coefficients of
+// x^t (t < kBlock) and the jump polynomials of every block a call of up to
+// kMaxVertices vertices can launch.  None of it depends on the seed or on V, so
+// it is written once per device and only read afterwards.  The copy is a plain
+// synchronous cudaMemcpy from host memory (no device allocation).
+sg_status setup_device(DeviceSetup &ds)
+{
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_color_scratch);
+    if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    std::vector<uint32_t> tab((size_t)kScratchWords);
+    Poly q(31, 0);
+    q[0] = 1;
+    for (int t = 0; t < kBlock; ++t) {
+        for (int i = 0; i < 31; ++i) tab[(size_t)i * kBlock + t] = q[i];
+        const uint32_t top = q[30];
+        for (int j = 30; j > 0; --j) q[j] = q[j - 1];
+        q[0] = top;
+        q[28] += top;
+    }
+    Poly J = xpow(341), step = xpow(kBlock);
+    for (int64_t b = 0; b < kMaxBlocks; ++b) {
+        std::memcpy(&tab[(size_t)(kCoefWords + b * 31)], J.data(), 31 * 4);
+        J = mulmod(J, step);
+    }
+    e = cudaMemcpy(p, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("scratch set-up: ") + cudaGetErrorString(e));
+    ds.scratch = (uint32_t *)p;
+    return SG_OK;
+}
+
 }  // namespace
 
 extern "C" sg_status sg_colors_noalloc(int32_t V, int32_t k, uint32_t seed, int32_t *d_colors, void *stream)
 {
-    if (V < 0 || V > kMaxVertices) {
-        return fail(SG_ERR_INVALID, "V must be in [0, 2^26] (the scratch array holds jump tables for 2^26 vertices)");
-    }
-    if (k < 1 || (V > 0 && !d_colors)) {
-        return fail(SG_ERR_INVALID, "k must be >= 1 and the output buffer non-null");
-    }
-    if (V == 0) return SG_OK;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) {
-        return fail(SG_ERR_CUDA, "no current CUDA device");
-    }
-    cudaStream_t st = (cudaStream_t)stream;
-    const int64_t nblocks = (V + kBlock - 1) / kBlock;
-    std::lock_guard<std::mutex> lk(g_mu);
-    if ((int)g_setup.size() <= dev) g_setup.resize(dev + 1);
-    DeviceSetup &ds = g_setup[dev];
-    if (!ds.scratch) {
-        // set-up once per device (with that device current): the host-side name of
-        // the array is not a device address, so take the address from the runtime
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_color_scratch);
-        if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        ds.scratch = (uint32_t *)p;
-    }
-    // every call writes the part of the scratch it reads: the coefficients of
-    // x^t (t < kBlock) and the jump polynomials of its blocks
-    std::vector<uint32_t> tab((size_t)(kCoefWords + nblocks * 31));
-    {
-        Poly q(31, 0);
-        q[0] = 1;
-        for (int t = 0; t < kBlock; ++t) {
-            for (int i = 0; i < 31; ++i) tab[(size_t)i * kBlock + t] = q[i];
-            const uint32_t top = q[30];
-            for (int j = 30; j > 0; --j) q[j] = q[j - 1];
-            q[0] = top;
-            q[28] += top;
+    try {
+        if (V < 0 || V > kMaxVertices) {
+            return fail(SG_ERR_INVALID,
+                        "V must be in [0, 2^26] (the scratch array holds jump tables for 2^26 vertices)");
         }
-        Poly J = xpow(341), step = xpow(kBlock);
-        for (int64_t b = 0; b < nblocks; ++b) {
-            std::memcpy(&tab[(size_t)(kCoefWords + b * 31)], J.data(), 31 * 4);
-            J = mulmod(J, step);
+        if (k < 1 || (V > 0 && !d_colors)) {
+            return fail(SG_ERR_INVALID, "k must be >= 1 and the output buffer non-null");
         }
+        if (V == 0) return SG_OK;
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) {
+            return fail(SG_ERR_CUDA, "no current CUDA device");
+        }
+        {
+            std::lock_guard<std::mutex> lk(g_mu);
+            if ((int)g_setup.size() <= dev) g_setup.resize(dev + 1);
+            if (!g_setup[dev].scratch) {
+                const sg_status st = setup_device(g_setup[dev]);
+                if (st != SG_OK) return st;
+            }
+        }
+        cudaStream_t st = (cudaStream_t)stream;
+        const int64_t nblocks = (V + kBlock - 1) / kBlock;
+        Window w0;
+        sg::glibc_window(seed, w0.w);
+        k_color_noalloc<<<(unsigned)nblocks, kBlock, 0, st>>>(V, k, w0, d_colors);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            return fail(SG_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+        }
+        return SG_OK;
+    } catch (const std::bad_alloc &) {
+        return fail(SG_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &ex) {
+        return fail(SG_ERR_CUDA, ex.what());
     }
-    cudaError_t e = cudaMemcpyAsync(ds.scratch, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return fail(SG_ERR_CUDA, std::string("table upload: ") + cudaGetErrorString(e));
-    Window w0;
-    sg::glibc_window(seed, w0.w);
-    k_color_noalloc<<<(unsigned)nblocks, kBlock, 0, st>>>(V, k, w0, d_colors);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) {
-        return fail(SG_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
-    }
-    return SG_OK;
 }

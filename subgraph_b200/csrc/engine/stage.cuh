@@ -7,7 +7,10 @@ namespace sg {
 enum CountMode : int32_t {
     kModeReference = 0,  // FP32 tables, the reference's arithmetic (isPruned=1)
     kModeFP64 = 1,       // FP64 tables, no scaling (the high-precision oracle mode)
-    kModeOriginal = 2,   // FP32 tables, isPruned=0 arithmetic (no scale, FP32 root)
+    kModeOriginal = 2,   // isPruned=0 on a CSC graph: FP32, no scale, FP32 root, and the SpMV
+                         // buffer accumulating over every split, sub and coloring (k_original)
+    kModeOriginalCSR = 3,  // isPruned=0 on a CSR graph: the same, with a fresh aggregation per
+                           // split (CSRGraph::SpMVNaiveFull overwrites its output)
 };
 
 // One sub-template step of nb colorings: the fused aggregation + eMA over all

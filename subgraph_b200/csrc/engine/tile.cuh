@@ -127,6 +127,38 @@ template <bool COH> __device__ __forceinline__ D4 ld_tab(const D4 *p)
     return r;
 }
 
+// The sum of n FP64 partials by one 256-thread block, in a fixed order with
+// Kahan compensation, times `scale` (valid in thread 0).  A non-finite sum
+// (an inf or NaN partial, which isPruned=0 runs reach) is returned as the
+// plain sum: compensation would turn inf into NaN.
+__device__ __forceinline__ double block_sum_partials(const double *p, int n, double scale, double *ss, double *cc,
+                                                     double *pp)
+{
+    double s = 0.0, c = 0.0, plain = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double x = p[i];
+        plain = __dadd_rn(plain, x);
+        const double y = __dadd_rn(x, -c);
+        const double t = __dadd_rn(s, y);
+        c = __dadd_rn(__dadd_rn(t, -s), -y);
+        s = t;
+    }
+    ss[threadIdx.x] = s;
+    cc[threadIdx.x] = c;
+    pp[threadIdx.x] = plain;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            ss[threadIdx.x] = __dadd_rn(ss[threadIdx.x], ss[threadIdx.x + w]);
+            cc[threadIdx.x] = __dadd_rn(cc[threadIdx.x], cc[threadIdx.x + w]);
+            pp[threadIdx.x] = __dadd_rn(pp[threadIdx.x], pp[threadIdx.x + w]);
+        }
+        __syncthreads();
+    }
+    const double r = isfinite(pp[0]) ? __dadd_rn(ss[0], -cc[0]) : pp[0];
+    return __dmul_rn(r, scale);
+}
+
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 

@@ -164,18 +164,61 @@ bool build_csc(int32_t V, const int32_t *src, const int32_t *dst, int64_t E, CSC
     return true;
 }
 
+void encode_graph_data(const CSC &g, std::string &buf)
+{
+    const size_t V = (size_t)g.V, nnz = g.indexRow.size();
+    buf.assign(8 + 4 * (V + V + 1 + 2 * nnz), '\0');
+    char *p = &buf[0];
+    const int32_t hdr[2] = {g.numEdges, g.V};
+    const float one = 1.0f;
+    std::memcpy(p, hdr, 8);
+    p += 8;
+    if (V) std::memcpy(p, g.degList.data(), 4 * V);
+    p += 4 * V;
+    std::memcpy(p, g.indexCol.data(), 4 * (V + 1));
+    p += 4 * (V + 1);
+    if (nnz) std::memcpy(p, g.indexRow.data(), 4 * nnz);
+    p += 4 * nnz;
+    for (size_t e = 0; e < nnz; ++e) std::memcpy(p + 4 * e, &one, 4);
+}
+
+bool decode_graph_data(const char *data, size_t n, const std::string &what, CSC &g, std::string &err)
+{
+    auto rd = [&](size_t off) { int32_t v; std::memcpy(&v, data + off, 4); return v; };
+    if (n < 8) { err = what + ": truncated header"; return false; }
+    int32_t ne = rd(0), V = rd(4);
+    if (V < 0) { err = what + ": negative vertex count"; return false; }
+    size_t off_deg = 8, off_col = off_deg + 4 * (size_t)V, off_row = off_col + 4 * ((size_t)V + 1);
+    if (n < off_row) { err = what + ": truncated offsets"; return false; }
+    int32_t nnz = rd(off_row - 4);
+    if (nnz < 0 || n != off_row + 8 * (size_t)nnz) {
+        err = what + ": size does not match numVertices/indexCol (expected " +
+              std::to_string(off_row + 8 * (size_t)(nnz < 0 ? 0 : nnz)) + " bytes, have " + std::to_string(n) + ")";
+        return false;
+    }
+    g.numEdges = ne;
+    g.V = V;
+    g.degList.resize((size_t)V);
+    g.indexCol.resize((size_t)V + 1);
+    g.indexRow.resize((size_t)nnz);
+    if (V) std::memcpy(g.degList.data(), data + off_deg, 4 * (size_t)V);
+    std::memcpy(g.indexCol.data(), data + off_col, 4 * ((size_t)V + 1));
+    if (nnz) std::memcpy(g.indexRow.data(), data + off_row, 4 * (size_t)nnz);
+    if (g.indexCol[0] != 0) { err = what + ": indexCol[0] != 0"; return false; }
+    for (int32_t i = 0; i < V; ++i)
+        if (g.indexCol[i + 1] < g.indexCol[i]) { err = what + ": indexCol not monotone"; return false; }
+    for (int32_t e = 0; e < nnz; ++e)
+        if (g.indexRow[e] < 0 || g.indexRow[e] >= V) { err = what + ": row id out of range"; return false; }
+    return true;
+}
+
 bool write_graph_data(const std::string &path, const CSC &g, std::string &err)
 {
+    std::string buf;
+    encode_graph_data(g, buf);
     FILE *f = std::fopen(path.c_str(), "wb");
     if (!f) { err = "cannot create " + path + ": " + std::strerror(errno); return false; }
-    int32_t hdr[2] = {g.numEdges, g.V};
-    size_t nnz = g.indexRow.size();
-    std::vector<float> vals(nnz, 1.0f);
-    bool ok = std::fwrite(hdr, 4, 2, f) == 2;
-    ok = ok && std::fwrite(g.degList.data(), 4, (size_t)g.V, f) == (size_t)g.V;
-    ok = ok && std::fwrite(g.indexCol.data(), 4, (size_t)g.V + 1, f) == (size_t)g.V + 1;
-    ok = ok && (nnz == 0 || std::fwrite(g.indexRow.data(), 4, nnz, f) == nnz);
-    ok = ok && (nnz == 0 || std::fwrite(vals.data(), 4, nnz, f) == nnz);
+    bool ok = std::fwrite(buf.data(), 1, buf.size(), f) == buf.size();
     ok = (std::fclose(f) == 0) && ok;
     if (!ok) err = "write failed on " + path;
     return ok;
@@ -185,33 +228,7 @@ bool read_graph_data(const std::string &path, CSC &g, std::string &err)
 {
     std::string buf;
     if (!slurp(path, buf, err)) return false;
-    const size_t n = buf.size();
-    auto rd = [&](size_t off) { int32_t v; std::memcpy(&v, buf.data() + off, 4); return v; };
-    if (n < 8) { err = path + ": truncated header"; return false; }
-    int32_t ne = rd(0), V = rd(4);
-    if (V < 0) { err = path + ": negative vertex count"; return false; }
-    size_t off_deg = 8, off_col = off_deg + 4 * (size_t)V, off_row = off_col + 4 * ((size_t)V + 1);
-    if (n < off_row) { err = path + ": truncated offsets"; return false; }
-    int32_t nnz = rd(off_row - 4);
-    if (nnz < 0 || n != off_row + 8 * (size_t)nnz) {
-        err = path + ": size does not match numVertices/indexCol (expected " +
-              std::to_string(off_row + 8 * (size_t)(nnz < 0 ? 0 : nnz)) + " bytes, have " + std::to_string(n) + ")";
-        return false;
-    }
-    g.numEdges = ne;
-    g.V = V;
-    g.degList.resize((size_t)V);
-    g.indexCol.resize((size_t)V + 1);
-    g.indexRow.resize((size_t)nnz);
-    if (V) std::memcpy(g.degList.data(), buf.data() + off_deg, 4 * (size_t)V);
-    std::memcpy(g.indexCol.data(), buf.data() + off_col, 4 * ((size_t)V + 1));
-    if (nnz) std::memcpy(g.indexRow.data(), buf.data() + off_row, 4 * (size_t)nnz);
-    if (g.indexCol[0] != 0) { err = path + ": indexCol[0] != 0"; return false; }
-    for (int32_t i = 0; i < V; ++i)
-        if (g.indexCol[i + 1] < g.indexCol[i]) { err = path + ": indexCol not monotone"; return false; }
-    for (int32_t e = 0; e < nnz; ++e)
-        if (g.indexRow[e] < 0 || g.indexRow[e] >= V) { err = path + ": row id out of range"; return false; }
-    return true;
+    return decode_graph_data(buf.data(), buf.size(), path, g, err);
 }
 
 namespace {

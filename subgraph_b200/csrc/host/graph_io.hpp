@@ -45,8 +45,13 @@ bool build_csr(int32_t V, const int32_t *src, const int32_t *dst, int64_t E, CSR
 // graph.data (CSCGraph::serialize/deserialize, CSCGraph.hpp:427-463): int32
 // numEdges, numVertices, degList[V], indexCol[V+1], indexRow[nnz], float
 // edgeVal[nnz] (all 1.0).
+// The CSR form (CSRGraph::serialize/deserialize, CSRGraph.cpp:236-295) is the
+// same layout with row offsets and column ids in place of indexCol/indexRow.
 bool write_graph_data(const std::string &path, const CSC &g, std::string &err);
 bool read_graph_data(const std::string &path, CSC &g, std::string &err);
+// the same bytes in memory (`what` names the source in error messages)
+void encode_graph_data(const CSC &g, std::string &buf);
+bool decode_graph_data(const char *data, size_t n, const std::string &what, CSC &g, std::string &err);
 
 // Seeded R-MAT / Kronecker generator: E = edge_factor * 2^scale draws with
 // initiator (a, b, c, 1-a-b-c), vertex ids scrambled by a seeded permutation,

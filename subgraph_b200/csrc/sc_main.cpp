@@ -1,4 +1,10 @@
-// sc-main: the reference's command line (sc-main.cpp:1556-1805) over the C ABI.
+// sc-main: the reference's command line (sc-main.cpp:1556-1805), written
+// against the C++ drop-in headers (include/subgraph_b200/*.hpp), which carry
+// the reference's class names and signatures over the C ABI.  The engine calls
+// below are the reference main's own sequence: EdgeList -> CSCGraph (or
+// CSRGraph)::createFromEdgeListFile -> splitCSC, or deserialize for
+// load_binary; serialize for write_binary; Graph::read_enlist;
+// CountMat::initialization; CountMat::compute.
 //
 //   sc-main graph template iterations threads load_binary write_binary
 //           [isPruned useSPMM vtuneStart benchItr]
@@ -8,28 +14,98 @@
 // the reference's: "Time for count per iter", "Final raw count is", "Prob is",
 // "Final count is".  Counting runs on CUDA device SG_DEVICE (default 0);
 // colorings are seeded srand(SG_SEED_BASE + c) when SG_SEED_BASE is set, else
-// from time(0) like the reference.  The reference's unrelated eMA triad
-// benchmark that precedes loading (sc-main.cpp:1606) is not run.
-#include <sys/time.h>
+// from time(0) like the reference.  The reference hard-codes the CSC graph
+// (useCSC, sc-main.cpp:1576); SG_USE_CSR=1 selects its CSRGraph branch.  The
+// reference's unrelated eMA triad benchmark that precedes loading
+// (sc-main.cpp:1606) is not run.
+#include <fcntl.h>
+#include <unistd.h>
 
 #include <cstdio>
 #include <cstdlib>
-#include <cstring>
+#include <fstream>
+#include <iostream>
 #include <string>
 
-#include "sg_api.h"
+#include "subgraph_b200/CountMat.hpp"
+#include "subgraph_b200/EdgeList.hpp"
 
-static double now()
+static int run(int argc, char **argv)
 {
-    struct timeval tp;
-    gettimeofday(&tp, nullptr);
-    return (double)tp.tv_sec + 1e-6 * (double)tp.tv_usec;
-}
+    const string graph_name = argv[1], template_name = argv[2];
+    const int iterations = std::atoi(argv[3]);
+    const int comp_thds = std::atoi(argv[4]);
+    const int load_binary = std::atoi(argv[5]);
+    const int write_binary = std::atoi(argv[6]);
+    const int isPruned = argc > 7 ? std::atoi(argv[7]) : 1;
+    const int useSPMM = argc > 8 ? std::atoi(argv[8]) : 1;
+    const int vtuneStart = argc > 9 ? std::atoi(argv[9]) : -1;
+    const bool calculate_automorphism = false;   // sc-main.cpp:1568
+    const bool useCSC = !(std::getenv("SG_USE_CSR") && std::atoi(std::getenv("SG_USE_CSR")));
+    const bool useMKL = false, useRcm = false;
+    if (iterations < 1) {
+        std::fprintf(stderr, "sc-main: iterations must be >= 1\n");
+        return 2;
+    }
 
-static int die(const char *what)
-{
-    std::fprintf(stderr, "sc-main: %s: %s\n", what, sg_last_error());
-    return 1;
+    CSRGraph *csrInputG = nullptr;
+    CSCGraph<int32_t, float> *cscInputG = nullptr;
+    if (!useCSC)
+        csrInputG = new CSRGraph();
+    else
+        cscInputG = new CSCGraph<int32_t, float>();
+    Graph input_template;
+
+    std::printf("Start loading datasets\n");
+    std::fflush(stdout);
+    double startTime = utility::timer();
+    if (load_binary) {
+        int input_file = open(graph_name.c_str(), O_RDONLY);
+        if (input_file < 0) throw sg_error(SG_ERR_IO, "cannot open " + graph_name);
+        if (csrInputG != nullptr) {
+            csrInputG->deserialize(input_file, useMKL, useRcm);
+        } else {
+            cscInputG->deserialize(input_file);
+            cscInputG->splitCSC(4 * comp_thds);
+        }
+        close(input_file);
+        std::printf("%s Format Total vertices is : %d\n", useCSC ? "CSC" : "CSR",
+                    useCSC ? cscInputG->getNumVertices() : csrInputG->getNumVertices());
+    } else {
+        double iotStart = utility::timer();
+        EdgeList elist(graph_name);
+        std::cout << "Disk Load Text Data using " << (utility::timer() - iotStart) << " s" << std::endl;
+        if (csrInputG != nullptr) {
+            csrInputG->createFromEdgeListFile(elist.getNumVertices(), elist.getNumEdges(), elist.getSrcList(),
+                                              elist.getDstList(), useMKL, useRcm, false);
+        } else {
+            cscInputG->createFromEdgeListFile(elist.getNumVertices(), elist.getNumEdges(), elist.getSrcList(),
+                                              elist.getDstList(), false);
+            cscInputG->splitCSC(4 * comp_thds);
+        }
+    }
+    if (write_binary) {
+        ofstream output_file("graph.data", ios::binary);
+        if (csrInputG != nullptr)
+            csrInputG->serialize(output_file);
+        else
+            cscInputG->serialize(output_file);
+        output_file.close();
+        if (!output_file) throw sg_error(SG_ERR_IO, "writing graph.data");
+    }
+    std::printf("Prepare Datasets using %f secs\n", utility::timer() - startTime);
+    std::fflush(stdout);
+
+    input_template.read_enlist(template_name);
+    CountMat executor;
+    executor.initialization(csrInputG, cscInputG, comp_thds, iterations, isPruned, useSPMM, vtuneStart,
+                            calculate_automorphism);
+    if (const char *s = std::getenv("SG_SEED_BASE")) executor.setSeed((uint32_t)std::strtoul(s, nullptr, 10));
+    executor.compute(input_template, false);
+
+    delete csrInputG;
+    delete cscInputG;
+    return 0;
 }
 
 int main(int argc, char **argv)
@@ -41,65 +117,10 @@ int main(int argc, char **argv)
                      argv[0]);
         return 2;
     }
-    const std::string graph_name = argv[1], template_name = argv[2];
-    const int iterations = std::atoi(argv[3]);
-    const int comp_thds = std::atoi(argv[4]);
-    const int load_binary = std::atoi(argv[5]);
-    const int write_binary = std::atoi(argv[6]);
-    const int isPruned = argc > 7 ? std::atoi(argv[7]) : 1;
-    const int useSPMM = argc > 8 ? std::atoi(argv[8]) : 1;
-    const int vtuneStart = argc > 9 ? std::atoi(argv[9]) : -1;
-    const bool calculate_automorphism = false;   // sc-main.cpp:1568
-    const int device = std::getenv("SG_DEVICE") ? std::atoi(std::getenv("SG_DEVICE")) : 0;
-    if (iterations < 1) {
-        std::fprintf(stderr, "sc-main: iterations must be >= 1\n");
-        return 2;
+    try {
+        return run(argc, argv);
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "sc-main: %s\n", e.what());
+        return 1;
     }
-
-    std::printf("Start loading datasets\n");
-    std::fflush(stdout);
-    double start = now();
-    int32_t V = 0, numEdges = 0;
-    int32_t *indexCol = nullptr, *indexRow = nullptr, *degList = nullptr;
-    if (load_binary) {
-        if (sg_graph_data_read(graph_name.c_str(), &V, &numEdges, &indexCol, &indexRow, &degList) != SG_OK)
-            return die("loading graph.data");
-        std::printf("CSC Format Total vertices is : %d\n", V);
-        std::printf("CSC Format Total Edges is : %d\n", numEdges);
-    } else {
-        int64_t E = 0;
-        int32_t *src = nullptr, *dst = nullptr;
-        std::printf("File name: %s\n", graph_name.c_str());
-        if (sg_edgelist_read(graph_name.c_str(), &V, &E, &src, &dst) != SG_OK) return die("reading the edge list");
-        std::printf("Vert: %d, Edge: %lld\n", V, (long long)E);
-        if (sg_csc_build(V, E, src, dst, &indexCol, &indexRow, &degList) != SG_OK) return die("building the CSC");
-        numEdges = (int32_t)E;
-        sg_free(src);
-        sg_free(dst);
-    }
-    if (write_binary && sg_graph_data_write("graph.data", V, numEdges, indexCol, indexRow, degList) != SG_OK)
-        return die("writing graph.data");
-    std::printf("Prepare Datasets using %f secs\n", now() - start);
-    std::fflush(stdout);
-
-    sg_plan tmpl = nullptr;
-    if (sg_plan_read(template_name.c_str(), &tmpl) != SG_OK) return die("reading the template");
-    sg_graph g = nullptr;
-    if (sg_graph_create(indexCol, indexRow, V, (int64_t)indexCol[V], device, &g) != SG_OK)
-        return die("uploading the graph");
-    sg_countmat cm = nullptr;
-    sg_countmat_create(&cm);
-    if (sg_countmat_initialization(cm, nullptr, g, comp_thds, iterations, isPruned, useSPMM, vtuneStart,
-                                   calculate_automorphism ? 1 : 0) != SG_OK)
-        return die("initialising the counter");
-    if (const char *s = std::getenv("SG_SEED_BASE")) sg_countmat_set_seed(cm, (uint32_t)std::strtoul(s, nullptr, 10));
-    double result = 0.0;
-    if (sg_countmat_compute(cm, tmpl, 0, 1, &result) != SG_OK) return die("counting");
-    sg_countmat_destroy(cm);
-    sg_graph_destroy(g);
-    sg_plan_destroy(tmpl);
-    sg_free(indexCol);
-    sg_free(indexRow);
-    sg_free(degList);
-    return 0;
 }

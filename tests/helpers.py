@@ -111,3 +111,63 @@ def has_gpu() -> bool:
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+@dataclass
+class FlagCase:
+    key: str
+    variant: str        # spmv | orig | csr_spmv | csr_orig
+    graph: str
+    template: str
+    n: int
+    edges: list
+    ncol: int
+    seed: int
+    V: int
+    csr: bool
+    is_pruned: int
+    use_spmm: int
+    raw: np.ndarray
+    colors: np.ndarray
+    table_sha: dict
+
+
+class GoldenFlags:
+    """The compiled reference's results for the CountMat flag variants and the
+    CSR input path (tests/golden/make_golden_flags.py)."""
+
+    def __init__(self):
+        self.meta = json.load(open(os.path.join(GOLDEN_DIR, "golden_flags.json")))
+        self.arr = dict(np.load(os.path.join(GOLDEN_DIR, "golden_flags.npz")))
+        self.cases = []
+        for m in self.meta["cases"]:
+            k = m["key"]
+            self.cases.append(FlagCase(
+                key=k, variant=m["variant"], graph=m["graph"], template=m["template"], n=m["n"],
+                edges=[tuple(e) for e in m["edges"]], ncol=m["ncol"], seed=m["seed"], V=m["V"], csr=m["csr"],
+                is_pruned=m["is_pruned"], use_spmm=m["use_spmm"], raw=self.arr[f"{k}_raw"],
+                colors=self.arr[f"{k}_colors"].astype(np.int32),
+                table_sha={int(a): b for a, b in m["table_sha"].items()}))
+
+    def edges(self, name):
+        g = self.meta["graphs"][name]
+        return g["V_declared"], self.arr[f"g_{name}_src"], self.arr[f"g_{name}_dst"]
+
+    def csr(self, name):
+        return self.arr[f"g_{name}_csr_row"], self.arr[f"g_{name}_csr_col"]
+
+
+def sha_nan(a: np.ndarray) -> str:
+    """SHA-256 of a float32 table with every NaN written as one canonical NaN."""
+    import hashlib
+    a = np.array(a, np.float32, copy=True)
+    a[np.isnan(a)] = np.float32("nan")
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def same_raw(a, b, tol=0.0) -> bool:
+    """Raw counts equal within a relative tolerance; inf and NaN must match."""
+    a, b = float(a), float(b)
+    if np.isnan(b) or np.isinf(b):
+        return (np.isnan(a) and np.isnan(b)) or a == b
+    return abs(a - b) <= tol * max(abs(b), 1e-300)

@@ -73,7 +73,7 @@ def test_batched_wait_timeout_is_an_error_and_context_survives(golden):
     g = _graph(golden, c.graph)
     t = sg.Graph(c.n, c.edges)
     with pytest.raises(sg.SGError) as e:
-        sg.count(g, t, 2, c.seed, batch=2, wait_limit_ms=200, test_unsatisfiable_wait=True, persistent=True)
+        sg.debug_count_unsatisfiable_wait(g, t, 2, c.seed, batch=2, wait_limit_ms=200)
     assert e.value.code == 4
     raw = sg.count(g, t, c.ncol, c.seed, batch=2, exact=True, persistent=True)
     assert all(rel(a, b) <= 1e-12 for a, b in zip(raw, c.raw))
@@ -103,7 +103,7 @@ def test_grouped_matches_plain_with_hubs_and_modes():
     g = csc.device_graph()
     for tname in ("spider7", "tree5", "tree12"):
         t = sg.Graph(*TEMPLATES[tname])
-        for mode in (sg.MODE_REFERENCE, sg.MODE_FP64, sg.MODE_ORIGINAL):
+        for mode in (sg.MODE_REFERENCE, sg.MODE_FP64, sg.MODE_ORIGINAL_CSR):
             n = 2 if tname == "tree12" else 9
             plain = sg.count(g, t, n, 21, mode=mode, hub_threshold=32, exact=True)
             grouped = sg.count(g, t, n, 21, mode=mode, hub_threshold=32, exact=True, batch=4)

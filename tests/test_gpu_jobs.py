@@ -56,7 +56,7 @@ def test_jobs_modes_and_hubs_match_plain(persistent):
     jobs = _jobs(rng, 12) + [TEMPLATES["tree12"]]
     tmpl = [sg.Graph(n, e) for n, e in jobs]
     seeds = list(range(40, 40 + len(jobs)))
-    for mode in (sg.MODE_REFERENCE, sg.MODE_FP64, sg.MODE_ORIGINAL):
+    for mode in (sg.MODE_REFERENCE, sg.MODE_FP64, sg.MODE_ORIGINAL_CSR):
         raw = sg.count_jobs(g, tmpl, seeds, mode=mode, exact=True, persistent=persistent)
         for j, (t, s) in enumerate(zip(tmpl, seeds)):
             assert rel(raw[j], sg.count(g, t, 1, s, mode=mode, exact=True)[0]) <= 1e-12, (mode, j)

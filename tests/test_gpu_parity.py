@@ -103,14 +103,17 @@ def test_fp64_mode_matches_oracle(golden):
         assert rel(raw[0], r64) <= 1e-12, (c.key, raw[0], r64)
 
 
-def test_original_mode_matches_oracle(golden):
+def test_original_modes_match_oracle(golden):
+    """isPruned=0: per-vertex root values of one coloring (from a zero SpMV
+    buffer in mode 2) identical to the oracle's, inf and NaN included."""
     for c in golden.cases[::4]:
         g, col, row = dev_graph(golden, c.graph)
         t = sg.Graph(c.n, c.edges)
         P = O.Plan(c.n, c.edges)
-        root, _ = sg.debug_root(g, t, c.seed, mode=sg.MODE_ORIGINAL, hub_threshold=0)
-        r, root_o = O.count_coloring(col, row, P, c.colors[0], mode=O.MODE_ORIGINAL, want_root=True)
-        assert np.array_equal(root, root_o), c.key
+        for mode, omode in ((sg.MODE_ORIGINAL, O.MODE_ORIGINAL), (sg.MODE_ORIGINAL_CSR, O.MODE_ORIGINAL_CSR)):
+            root, _ = sg.debug_root(g, t, c.seed, mode=mode, hub_threshold=0)
+            r, root_o = O.count_coloring(col, row, P, c.colors[0], mode=omode, want_root=True)
+            assert np.array_equal(root, root_o, equal_nan=True), (c.key, mode)
 
 
 def test_k2_template_keeps_reference_scaling(golden):

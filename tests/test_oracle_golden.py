@@ -117,3 +117,41 @@ def test_planted_mistake_is_caught(golden):
     hub = int(np.argmax(np.diff(col)))
     colors[hub] = (colors[hub] + 1) % c.n
     assert O.count_coloring(col, row, P, colors) != c.raw[0]
+
+
+# ---------------------------------------------------------------------------
+# CountMat flag variants and the CSR input path (golden_flags: the compiled
+# reference with isPruned / useSPMM / CSRGraph)
+# ---------------------------------------------------------------------------
+def test_oracle_flag_variants_match_reference():
+    from tests.helpers import GoldenFlags, same_raw
+    gf = GoldenFlags()
+    modes = {"spmv": O.MODE_REF, "orig": O.MODE_ORIGINAL, "csr_spmv": O.MODE_REF, "csr_orig": O.MODE_ORIGINAL_CSR}
+    for c in gf.cases:
+        V, src, dst = gf.edges(c.graph)
+        if c.csr:
+            off, nbr = gf.csr(c.graph)
+        else:
+            off, nbr, _ = O.csc_build(V, src, dst)
+        assert np.array_equal(c.colors[0], O.colors(c.seed, c.V, c.n))
+        P = O.Plan(c.n, c.edges)
+        raw = O.count_colorings(off, nbr, P, [c.colors[i] for i in range(c.ncol)], modes[c.variant])
+        for i in range(c.ncol):
+            assert same_raw(raw[i], c.raw[i]), (c.variant, c.graph, c.template, i, raw[i], c.raw[i])
+
+
+def test_useSPMM_flag_does_not_change_results(golden):
+    """countNonBottomePruned (useSPMM=0) equals countNonBottomePrunedSPMM bit for
+    bit in the reference: same graph, template and seeds in both fixture sets."""
+    from tests.helpers import GoldenFlags
+    gf = GoldenFlags()
+    n = 0
+    for c in gf.cases:
+        if c.variant != "spmv":
+            continue
+        for g in golden.cases:
+            if g.graph == c.graph and g.template == c.template and g.seed == c.seed:
+                m = min(g.ncol, c.ncol)
+                assert np.array_equal(g.raw[:m], c.raw[:m]), (c.graph, c.template)
+                n += 1
+    assert n >= 3
