@@ -171,6 +171,9 @@ typedef struct {
     int32_t persistent;     /* batched form: 1 = one persistent work-queue launch per batch
                                (colorings in separate table slots); 0 = interleaved groups
                                (the batch's colorings share table rows and neighbour passes) */
+    int32_t no_rooted;      /* 1: no rooted form of the register-blocked eMA (a vertex of color c
+                               computes only the outputs and products whose sets hold c, over
+                               the other k-1 colors); the two give identical values */
 } sg_count_opts;
 
 typedef struct {

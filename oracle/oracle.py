@@ -204,7 +204,7 @@ def run_ref(graph_txt: str, template: str, ncol: int, seed: int, outdir: str, th
                            "1" if dump_tables else "0", "1" if automorphisms else "0", str(is_pruned),
                            str(use_spmm), "1" if csr else "0", "1" if light else "0"],
                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
-                          env=dict(os.environ, OMP_NUM_THREADS="1"))
+                          env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
     return load_ref_dump(outdir)
 
 

@@ -9,8 +9,7 @@
 // (CountMat.cpp:984).  This file defines time() so that coloring c of a run
 // with base seed S sees time() == S + c, and the coloring region runs on one
 // OpenMP thread, which makes the reference's coloring the glibc stream of
-// srand(S + c).  The counting loops still use `threads` threads (they take
-// num_threads(thd_num) explicitly).
+// srand(S + c).  Every other parallel region runs on `threads` threads.
 //
 // Usage: ref_oracle <graph.txt> <template> <ncolorings> <seed_base> <threads>
 //                   <outdir> [dump_tables] [automorphisms] [isPruned] [useSPMM]
@@ -63,12 +62,19 @@ static void write_bin(const std::string &path, const void *p, size_t bytes)
     fclose(f);
 }
 
-// One coloring, restating colorCounting (CountMat.cpp:268-322) step by step so
-// that every sub-template table can be copied out right after it is computed
-// (its parent later overwrites it in place with the aggregation).
-static double counting_with_dump(CountMat &cm, const std::string &dir)
+// One coloring: colorCounting (CountMat.cpp:268-322) step by step, with the
+// reference's own per-step functions, so that (i) the coloring runs on one
+// OpenMP thread (deterministic glibc stream) while every other parallel region
+// -- several use omp_get_max_threads(), e.g. the SpMM transposes at
+// CountMat.cpp:699-730 -- runs on `thds` threads, and (ii) with `dump` every
+// sub-template table can be copied out right after it is computed (its parent
+// later overwrites it in place with the aggregation).  The per-sub
+// "Mem utilization" report line and its /proc read are left out.
+static double counting(CountMat &cm, const std::string &dir, bool dump, int thds)
 {
+    omp_set_num_threads(1);
     cm.colorInit();
+    omp_set_num_threads(thds);
     double countTotal = 0.0;
     cm._isScaled = 0;
     int V = cm._vert_num;
@@ -84,7 +90,7 @@ static double counting_with_dump(CountMat &cm, const std::string &dir)
             countTotal = cm._useSPMM == 1 ? cm.countNonBottomePrunedSPMM(s) : cm.countNonBottomePruned(s);
         else
             countTotal = cm.countNonBottomeOriginal(s);
-        if (s > 0 && (subSize > 1 || s == cm._total_sub_num - 1)) {
+        if (dump && s > 0 && (subSize > 1 || s == cm._total_sub_num - 1)) {
             int L = cm._dTable.getTableLen(s);
             std::vector<float> buf((size_t)L * V);
             for (int c = 0; c < L; ++c)
@@ -144,7 +150,7 @@ int main(int argc, char **argv)
     Graph input_template;
     input_template.read_enlist(tmpl);
 
-    omp_set_num_threads(1);
+    omp_set_num_threads(thds);
     CountMat cm;
     cm.initialization(use_csr ? &csr : nullptr, use_csr ? nullptr : &csc, thds, ncol, is_pruned, use_spmm, -1, false);
 
@@ -204,14 +210,12 @@ int main(int argc, char **argv)
     for (int c = 0; c < ncol; ++c) {
         g_time_base = seed + c;
         const double t0 = omp_get_wtime();
-        double raw;
-        if (c == 0 && dump_tables) {
-            raw = counting_with_dump(cm, dir);
+        const bool dump = c == 0 && dump_tables;
+        const double raw = counting(cm, dir, dump, thds);
+        if (dump) {
             FILE *f = fopen((dir + "/raw_dump.txt").c_str(), "w");
             fprintf(f, "%.17g\n", raw);
             fclose(f);
-        } else {
-            raw = cm.colorCounting();  // the reference's own per-coloring function
         }
         const double t1 = omp_get_wtime();
         if (!light) std::memcpy(&colors[(size_t)c * V], cm._colors_local, sizeof(int32_t) * V);

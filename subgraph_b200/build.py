@@ -25,7 +25,7 @@ CXX_FLAGS = ["-std=c++17", "-O3", "-fPIC", "-Wall", "-Wno-unused-function"]
 
 HOST_SOURCES = ["host/graph_io.cpp", "host/plan.cpp", "capi.cpp"]
 CUDA_SOURCES = ["engine/kernels.cu", "engine/blocked.cu", "engine/blocked_a.cu", "engine/blocked_b.cu",
-                "engine/blocked_c.cu", "engine/blocked_d.cu", "engine/engine.cu", "engine/batch.cu", "engine/noalloc.cu",
+                "engine/blocked_c.cu", "engine/blocked_d.cu", "engine/blocked_e.cu", "engine/engine.cu", "engine/batch.cu", "engine/noalloc.cu",
                 "engine/input_gpu.cu"]
 
 

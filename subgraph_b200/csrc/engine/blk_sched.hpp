@@ -94,14 +94,19 @@ template <int N, int P> struct Sched {
     static constexpr Table<N, P> tab = make_table<N, P>();
 };
 
-// The shapes with a blocked kernel: (N, P) with P >= 2 (a one-hot main has its
-// own path), N <= 11, at most 64 held values.  Index 0 means "no blocked
-// path"; shape ids are 1 + the position in this list.
+// The shapes with a blocked kernel: (N, P) with N <= 11 and at most 64 held
+// values.  P >= 2 for a sub's own split structure (a one-hot main has its own
+// path); the P = 1 shapes serve the rooted form, where a stage of shape
+// (N + 1, P + 1) is computed per vertex over the other k - 1 colors and its
+// main operands (the sets holding the vertex's color) are not one-hot.
+// Index 0 means "no blocked path"; shape ids are 1 + the position in this list.
 #define SG_BLK_SHAPES_A(X) X(3, 2) X(4, 2) X(4, 3) X(5, 2) X(5, 3) X(5, 4) X(6, 2) X(6, 3)
 #define SG_BLK_SHAPES_B(X) X(6, 4) X(6, 5) X(7, 2) X(7, 3) X(7, 4) X(7, 5)
 #define SG_BLK_SHAPES_C(X) X(7, 6) X(8, 2) X(8, 6) X(8, 7) X(9, 2) X(9, 7)
 #define SG_BLK_SHAPES_D(X) X(9, 8) X(10, 2) X(10, 8) X(10, 9) X(11, 10)
-#define SG_BLK_SHAPES(X) SG_BLK_SHAPES_A(X) SG_BLK_SHAPES_B(X) SG_BLK_SHAPES_C(X) SG_BLK_SHAPES_D(X)
+#define SG_BLK_SHAPES_E(X) X(2, 1) X(3, 1) X(4, 1) X(5, 1) X(6, 1) X(7, 1) X(8, 1) X(9, 1) X(10, 1)
+#define SG_BLK_SHAPES(X) \
+    SG_BLK_SHAPES_A(X) SG_BLK_SHAPES_B(X) SG_BLK_SHAPES_C(X) SG_BLK_SHAPES_D(X) SG_BLK_SHAPES_E(X)
 
 // Runtime view of one shape's schedule (host planner).
 struct View {

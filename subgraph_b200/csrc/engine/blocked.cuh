@@ -2,8 +2,8 @@
 // kernel per blocked shape (|s|, |main|): each kernel's register allocation
 // is that of its own schedule, so shapes with few held values and
 // accumulators run two CTAs per SM.  Gather and main-row phases are those of
-// fused_tile.  The shapes are instantiated in four translation units
-// (blocked_a.cu ... blocked_d.cu) that compile in parallel.
+// fused_tile.  The shapes are instantiated in five translation units
+// (blocked_a.cu ... blocked_e.cu) that compile in parallel.
 #pragma once
 #include "kernels.cuh"
 #include "tile.cuh"
@@ -22,7 +22,7 @@ __global__ void __launch_bounds__(NT, (NT == 512 ? blk_min_blocks<N, P>() : 2 * 
     k_fused_blk(StageDesc d)
 {
     extern __shared__ __align__(32) unsigned char smem_raw[];
-    for (int tile = blockIdx.x; tile < d.ntiles; tile += gridDim.x)
+    for (int tile = d.tile_begin + blockIdx.x; tile < d.ntiles; tile += gridDim.x)
         fused_tile<float, NT, Q, false, false, true, N, P>(d, tile, smem_raw);
 }
 
@@ -34,7 +34,7 @@ static void launch_blk_q(const StageDesc &d, const FusedConfig &cfg, cudaStream_
         int per_sm = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, cfg.smem) != cudaSuccess || per_sm < 1)
             per_sm = 1;
-        const int grid = std::max(1, std::min(d.ntiles, cfg.grid * per_sm));
+        const int grid = std::max(1, std::min(d.ntiles - d.tile_begin, cfg.grid * per_sm));
         kern<<<grid, NT, cfg.smem, st>>>(d);
     };
     switch (d.gather_q) {

@@ -105,6 +105,8 @@ struct Workspace {
     size_t adjc_bytes = 0;
     float *orig_buf = nullptr;         // [V] isPruned=0 (CSC) aggregation buffer, internal order
     size_t orig_buf_bytes = 0;
+    int32_t *hub_err = nullptr;        // set by the exact-order hub kernel when a bounded wait runs out
+    size_t hub_err_bytes = 0;
     uint64_t generation = 0;   // bumped whenever a buffer above is re-allocated
 };
 
@@ -115,6 +117,11 @@ struct DevicePlanTables {
     std::vector<uint32_t *> aoff, moff;  // per sub: packed-layout byte offsets (FP32)
     std::vector<int32_t *> blk;      // per sub: register-blocked eMA column tables, or null
     std::vector<int32_t> blk_shape, blk_nblocks;
+    // per sub: the rooted form (StageDesc::rooted), or null
+    std::vector<int32_t *> rblk;
+    std::vector<int32_t> rblk_shape, rblk_nblocks, r_Ls, r_La, r_Lm;
+    std::vector<uint32_t *> agg_chunk;
+    std::vector<int16_t *> main_full, out_rank;
     // per sub with a non-leaf aux child: [k][chunks] masks for 32-byte chunks (8 FP32 / 4 FP64 columns)
     std::vector<uint16_t *> cmask_f32, cmask_f64;
     std::vector<int32_t> cmf32_stride, cmf64_stride;
@@ -147,6 +154,10 @@ void free_batch(BatchPlan &b, cudaStream_t stream)
 
 struct GraphState {
     Workspace ws;
+    // the exact-order hub kernel runs on this stream while the tiles without
+    // hubs run on the caller's (events: stage inputs ready, hub rows ready)
+    cudaStream_t hub_stream = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_hub = nullptr;
     std::map<uint64_t, DevicePlanTables> plans;
     std::map<std::string, BatchPlan> batches; // batch shape -> work queue
     std::vector<cudaStream_t> streams;        // job streams (created on first use)
@@ -167,6 +178,7 @@ std::mutex g_state_mu;
 // handle of the same CSC arrays, as the end-to-end path creates per call)
 // reuses them.  Key: graph signature | stage shape.
 std::map<std::string, TileShape> g_tuned;
+std::map<std::string, int> g_hub_tuned;   // exact-order hub kernel variant per graph | row width
 
 std::string graph_sig(const DeviceGraph &g)
 {
@@ -221,12 +233,32 @@ template <typename T> Status growT(T **p, size_t *have, size_t need, cudaStream_
 // output's product sequence under the block schedule is checked against the
 // split tables (main_split/aux_split in split order); any difference, or a
 // shape without a blocked kernel, leaves the sub on the per-output loop.
+// The tables of an index structure: k colors, outputs of n colors, mains of
+// pm colors (a sub's own, or the rooted one over k - 1 colors).
+struct IndexView {
+    int k, n, pm, L, S;
+    const int32_t *comb_to_count, *main_split, *aux_split;
+};
+
+bool build_blocks(const IndexView &st, std::vector<int32_t> &rows, int &nblocks, int &shape);
+
 bool build_blocks(const Plan &p, int s, std::vector<int32_t> &rows, int &nblocks, int &shape)
 {
     const SubTemplate &st = p.subs[s];
-    const int k = p.k, n = st.size, pm = p.subs[st.main].size;
+    const int pm = p.subs[st.main].size;
     nblocks = 0;
-    shape = (s == 0 || pm < 2 || n + 1 > k) ? 0 : blk::shape_id(n, pm);
+    shape = 0;
+    if (s == 0 || pm < 2) return false;
+    const IndexView iv{p.k, st.size, pm, st.L, st.S, st.comb_to_count.data(), st.main_split.data(),
+                       st.aux_split.data()};
+    return build_blocks(iv, rows, nblocks, shape);
+}
+
+bool build_blocks(const IndexView &st, std::vector<int32_t> &rows, int &nblocks, int &shape)
+{
+    const int k = st.k, n = st.n, pm = st.pm;
+    nblocks = 0;
+    shape = (pm < 1 || n + 1 > k) ? 0 : blk::shape_id(n, pm);
     blk::View v;
     if (!shape || !blk::view_by_id(shape, v)) return false;
     auto colex = [&](unsigned mask) {
@@ -354,8 +386,90 @@ Status upload_chunk_masks(DeviceGraph &g, const Plan &p, int s, DevicePlanTables
     return Status::ok();
 }
 
+// The rooted form of sub s (main and aux of two colors or more): the index
+// structure of a stage of |s|-1 colors with mains of |main|-1 over k-1 colors,
+// its register-blocked tables, and per vertex color c the compaction tables:
+// the rank of every aggregate column lacking c (per 8-column chunk: the first
+// rank and the mask of such columns), the table column of every rooted main
+// set (the sets holding c, in colex order), and the rooted rank of every
+// output column holding c.  Colex order restricted to the sets lacking (or
+// holding) c is the colex order of those sets with c removed and the colors
+// above c renumbered, so each rank is the count of such columns before it.
+Status upload_rooted(DeviceGraph &g, const Plan &p, int s, DevicePlanTables &out)
+{
+    const SubTemplate &st = p.subs[s];
+    const SubTemplate &m = p.subs[st.main], &a = p.subs[st.aux];
+    const int k = p.k, n = st.size, pm = m.size, na = a.size;
+    if (s == 0 || pm < 2 || na < 2 || k < 3) return Status::ok();
+    int L = 0, S = 0;
+    std::vector<int32_t> c2c, ms, as;
+    index_tables(k - 1, n - 1, pm - 1, L, S, c2c, ms, as);
+    const IndexView iv{k - 1, n - 1, pm - 1, L, S, c2c.data(), ms.data(), as.data()};
+    std::vector<int32_t> rows;
+    int nb = 0, shape = 0;
+    if (!build_blocks(iv, rows, nb, shape)) return Status::ok();
+    auto mask_of = [&](int size, int col) {
+        int el[32];
+        colex_unrank(size, col, el);
+        unsigned msk = 0;
+        for (int i = 0; i < size; ++i) msk |= 1u << el[i];
+        return msk;
+    };
+    const int La = a.L, Lm = m.L, Ls = st.L, nch = (La + 7) / 8;
+    const int rLa = (int)binom(k - 1, na), rLm = (int)binom(k - 1, pm - 1);
+    std::vector<uint32_t> ach((size_t)k * nch, 0u);
+    std::vector<int16_t> mf((size_t)k * rLm, 0), orank((size_t)k * Ls, -1);
+    std::vector<unsigned> amask(La), mmask(Lm), omask(Ls);
+    for (int t = 0; t < La; ++t) amask[t] = mask_of(na, t);
+    for (int t = 0; t < Lm; ++t) mmask[t] = mask_of(pm, t);
+    for (int t = 0; t < Ls; ++t) omask[t] = mask_of(n, t);
+    for (int c = 0; c < k; ++c) {
+        int rank = 0;
+        for (int q = 0; q < nch; ++q) {
+            uint32_t lack = 0;
+            const int base = rank;
+            for (int i = 0; i < 8; ++i) {
+                const int t = q * 8 + i;
+                if (t < La && !(amask[t] >> c & 1u)) { lack |= 1u << i; ++rank; }
+            }
+            ach[(size_t)c * nch + q] = (uint32_t)base | lack << 16;
+        }
+        int r = 0;
+        for (int t = 0; t < Lm; ++t)
+            if (mmask[t] >> c & 1u) mf[(size_t)c * rLm + r++] = (int16_t)t;
+        int o = 0;
+        for (int t = 0; t < Ls; ++t)
+            if (omask[t] >> c & 1u) orank[(size_t)c * Ls + t] = (int16_t)o++;
+        if (rank != rLa || r != rLm || o != L) return Status{1, "rooted tables: column counts do not match"};
+    }
+    SG_CK(cudaMallocAsync(&out.rblk[s], rows.size() * 4, g.stream));
+    SG_CK(cudaMallocAsync(&out.agg_chunk[s], ach.size() * 4, g.stream));
+    SG_CK(cudaMallocAsync(&out.main_full[s], mf.size() * 2, g.stream));
+    SG_CK(cudaMallocAsync(&out.out_rank[s], orank.size() * 2, g.stream));
+    SG_CK(cudaMemcpyAsync(out.rblk[s], rows.data(), rows.size() * 4, cudaMemcpyHostToDevice, g.stream));
+    SG_CK(cudaMemcpyAsync(out.agg_chunk[s], ach.data(), ach.size() * 4, cudaMemcpyHostToDevice, g.stream));
+    SG_CK(cudaMemcpyAsync(out.main_full[s], mf.data(), mf.size() * 2, cudaMemcpyHostToDevice, g.stream));
+    SG_CK(cudaMemcpyAsync(out.out_rank[s], orank.data(), orank.size() * 2, cudaMemcpyHostToDevice, g.stream));
+    SG_CK(cudaStreamSynchronize(g.stream));   // the host vectors go out of scope
+    out.rblk_shape[s] = shape;
+    out.rblk_nblocks[s] = nb;
+    out.r_Ls[s] = L;
+    out.r_La[s] = rLa;
+    out.r_Lm[s] = rLm;
+    return Status::ok();
+}
+
 Status upload_plan(DeviceGraph &g, const Plan &p, DevicePlanTables &out)
 {
+    out.rblk.assign(p.nsub(), nullptr);
+    out.rblk_shape.assign(p.nsub(), 0);
+    out.rblk_nblocks.assign(p.nsub(), 0);
+    out.r_Ls.assign(p.nsub(), 0);
+    out.r_La.assign(p.nsub(), 0);
+    out.r_Lm.assign(p.nsub(), 0);
+    out.agg_chunk.assign(p.nsub(), nullptr);
+    out.main_full.assign(p.nsub(), nullptr);
+    out.out_rank.assign(p.nsub(), nullptr);
     out.cmask_f32.assign(p.nsub(), nullptr);
     out.cmask_f64.assign(p.nsub(), nullptr);
     out.cmf32_stride.assign(p.nsub(), 0);
@@ -423,6 +537,7 @@ Status upload_plan(DeviceGraph &g, const Plan &p, DevicePlanTables &out)
             SG_CK(cudaMemcpyAsync(out.rem[s], rem.data(), rem.size() * 2, cudaMemcpyHostToDevice, g.stream));
         }
         SG_CKS(upload_chunk_masks(g, p, s, out));
+        SG_CKS(upload_rooted(g, p, s, out));
     }
     SG_CK(cudaStreamSynchronize(g.stream));
     return Status::ok();
@@ -430,16 +545,21 @@ Status upload_plan(DeviceGraph &g, const Plan &p, DevicePlanTables &out)
 
 struct Hubs {
     int32_t count = 0, chunk = 0, total_chunks = 0;
+    bool exact_order = false;
 };
 
 // Vertices of degree above `thr` (the first `count` of the degree-descending
-// order) are aggregated in neighbour chunks of `thr` neighbours, one hub item
-// each.
-Hubs plan_hubs(const DeviceGraph &g, int thr)
+// order) are aggregated by the hub kernel.  In exact order each hub is one
+// chunk, summed in neighbour-list order with its columns split among lanes
+// (the same sums as the per-tile aggregation); otherwise in neighbour chunks
+// of `thr` neighbours, one hub item each, whose partial rows are added in
+// chunk order (another summation order).
+Hubs plan_hubs(const DeviceGraph &g, int thr, bool exact_order)
 {
     Hubs h;
     if (thr <= 0) return h;
-    h.chunk = thr;
+    h.exact_order = exact_order;
+    h.chunk = exact_order ? std::max(thr, g.max_degree) : thr;
     while (h.count < g.V && g.h_degree[h.count] > thr) {
         h.total_chunks += (g.h_degree[h.count] + h.chunk - 1) / h.chunk;
         ++h.count;
@@ -460,7 +580,8 @@ DeviceGraph::~DeviceGraph()
         if (it != g_state.end()) {
             Workspace &w = it->second.ws;
             for (void *p : {w.arena, (void *)w.colors, (void *)w.partial, (void *)w.raw, (void *)w.windows, w.hub_partial,
-                            (void *)w.chunk_start, (void *)w.root_vertex, (void *)w.adjc, (void *)w.orig_buf})
+                            (void *)w.chunk_start, (void *)w.root_vertex, (void *)w.adjc, (void *)w.orig_buf,
+                            (void *)w.hub_err})
                 if (p) cudaFreeAsync(p, stream);
             for (auto &kv : it->second.plans) {
                 for (auto *p : kv.second.split) if (p) cudaFreeAsync(p, stream);
@@ -468,6 +589,10 @@ DeviceGraph::~DeviceGraph()
                 for (auto *p : kv.second.rem) if (p) cudaFreeAsync(p, stream);
                 for (auto *p : kv.second.aoff) if (p) cudaFreeAsync(p, stream);
                 for (auto *p : kv.second.blk) if (p) cudaFreeAsync(p, stream);
+                for (auto *p : kv.second.rblk) if (p) cudaFreeAsync(p, stream);
+                for (auto *p : kv.second.agg_chunk) if (p) cudaFreeAsync(p, stream);
+                for (auto *p : kv.second.main_full) if (p) cudaFreeAsync(p, stream);
+                for (auto *p : kv.second.out_rank) if (p) cudaFreeAsync(p, stream);
                 for (auto *p : kv.second.moff) if (p) cudaFreeAsync(p, stream);
                 for (auto *p : kv.second.cmask_f32) if (p) cudaFreeAsync(p, stream);
                 for (auto *p : kv.second.cmask_f64) if (p) cudaFreeAsync(p, stream);
@@ -477,6 +602,12 @@ DeviceGraph::~DeviceGraph()
                 cudaStreamSynchronize(js);
                 cudaStreamDestroy(js);
             }
+            if (it->second.hub_stream) {
+                cudaStreamSynchronize(it->second.hub_stream);
+                cudaStreamDestroy(it->second.hub_stream);
+            }
+            if (it->second.ev_in) cudaEventDestroy(it->second.ev_in);
+            if (it->second.ev_hub) cudaEventDestroy(it->second.ev_hub);
             g_state.erase(it);
         }
     }
@@ -614,6 +745,7 @@ struct RunCtx {
     bool profile = false;
     bool autotune = false;
     bool blocked = true;     // register-blocked eMA allowed
+    bool rooted = true;      // its rooted form allowed
     int lay = 1;             // colorings interleaved per table row (grouped batched form)
     size_t arena_base = 0;   // byte offset of this context's tables in the arena (job queues)
     bool exact = false;      // no fused products (packed eMA), no hub chunks
@@ -686,6 +818,10 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
     SG_CKS(growT(&w.windows, &w.windows_bytes, 4 * 31 * (size_t)std::max(ncolorings_total, 1), g.stream));
     if (c.use_adjc) SG_CKS(growT(&w.adjc, &w.adjc_bytes, std::max<size_t>(16, 4 * (size_t)g.nnz), g.stream));
     if (c.mode == kModeOriginal) SG_CKS(growT(&w.orig_buf, &w.orig_buf_bytes, std::max<size_t>(16, 4 * V), g.stream));
+    if (c.hubs.exact_order && c.hubs.count > 0) {
+        SG_CKS(growT(&w.hub_err, &w.hub_err_bytes, 16, g.stream));
+        SG_CK(cudaMemsetAsync(w.hub_err, 0, 4, g.stream));
+    }
     if (c.hubs.count > 0) {
         // a partial row holds the aux columns (or colour counts) of up to c.lay colorings
         int32_t maxp = round_up(c.lay * c.p.k, 8);
@@ -701,6 +837,17 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
         SG_CKS(growT(&w.chunk_start, &w.chunk_start_bytes, 4 * cs.size(), g.stream));
         SG_CK(cudaMemcpyAsync(w.chunk_start, cs.data(), 4 * cs.size(), cudaMemcpyHostToDevice, g.stream));
     }
+    return Status::ok();
+}
+
+// After the stream is synchronised: the exact-order hub kernel's error flag
+// (a bounded wait that ran out) as a status.
+Status hub_status(GraphState &gs, const Hubs &hubs)
+{
+    if (!hubs.exact_order || hubs.count == 0 || !gs.ws.hub_err) return Status::ok();
+    int32_t e = 0;
+    SG_CK(cudaMemcpy(&e, gs.ws.hub_err, 4, cudaMemcpyDeviceToHost));
+    if (e) return Status{4, "exact-order hub aggregation: a bounded wait ran out"};
     return Status::ok();
 }
 
@@ -766,6 +913,22 @@ StageDesc make_stage(RunCtx &c, int slot, int s, double *root_vertex, int b0 = 0
     d.blk = (c.fp64 || !c.blocked) ? nullptr : c.tab->blk[s];
     d.blk_shape = d.blk ? c.tab->blk_shape[s] : 0;
     d.blk_nblocks = d.blk ? c.tab->blk_nblocks[s] : 0;
+    d.ublk = d.blk;
+    d.ublk_shape = d.blk_shape;
+    d.ublk_nblocks = d.blk_nblocks;
+    // the rooted form skips exact-zero products: FP32 reference arithmetic only
+    // (isPruned=0 tables may hold inf, where a skipped 0 * inf would be NaN)
+    if (!c.fp64 && c.blocked && c.rooted && c.mode == kModeReference && L == 1 && nb == 1 && c.tab->rblk[s]) {
+        d.rblk = c.tab->rblk[s];
+        d.rblk_shape = c.tab->rblk_shape[s];
+        d.rblk_nblocks = c.tab->rblk_nblocks[s];
+        d.r_Ls = c.tab->r_Ls[s];
+        d.r_La = c.tab->r_La[s];
+        d.r_Lm = c.tab->r_Lm[s];
+        d.agg_chunk = c.tab->agg_chunk[s];
+        d.main_full = c.tab->main_full[s];
+        d.out_rank = c.tab->out_rank[s];
+    }
     d.color = w.colors + (size_t)slot * g.V + b0;
     if (c.use_adjc && L == 1) {
         d.adjc = w.adjc + (size_t)slot * g.nnz;
@@ -796,6 +959,9 @@ HubArgs make_hub(RunCtx &c, StageDesc &d, void *partial)
     h.color = d.color;
     h.total_chunks = c.hubs.total_chunks;
     h.chunk_start = c.gs.ws.chunk_start;
+    h.exact_order = c.hubs.exact_order ? 1 : 0;
+    h.err = c.gs.ws.hub_err;
+    h.wait_cycles = 4000000000LL;   // about 2 s at the maximum SM clock
     h.off = g.d_off;
     h.adj = g.d_adj;
     h.aux = d.aux;
@@ -849,14 +1015,68 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
     if (c.mode == kModeOriginal) return run_stage_original(c, slot, s, root_vertex, st);
     DeviceGraph &g = c.g;
     StageDesc d = make_stage(c, slot, s, root_vertex, b0, nb);
+    bool side = false;   // hub rows come from the side stream (event ev_hub)
     if (c.hubs.count > 0) {
         HubArgs h = make_hub(c, d, c.hub_region ? c.hub_region : c.gs.ws.hub_partial);
+        int variant = 0;
+        if (h.exact_order && !h.k_leaf) {
+            // the exact-order hub kernel's (threads, ring depth) pair: timed once per
+            // graph and row width (all variants compute the same rows)
+            const std::string key = graph_sig(g) + "hub/" + std::to_string(h.L_a) + "/" + std::to_string(h.hub_count) +
+                                    "/" + std::to_string((int)c.fp64);
+            bool have = false;
+            {
+                std::lock_guard<std::mutex> lk(g_state_mu);
+                auto it = g_hub_tuned.find(key);
+                if (it != g_hub_tuned.end()) { variant = it->second; have = true; }
+            }
+            if (!have && c.autotune) {
+                cudaEvent_t e0, e1;
+                SG_CK(cudaEventCreate(&e0));
+                SG_CK(cudaEventCreate(&e1));
+                float best = 1e30f;
+                for (int vv = 0; vv < hub_variants(); ++vv) {
+                    launch_hub(h, c.fp64, g.sm_count, st, vv);   // untimed: module load
+                    SG_CK(cudaEventRecord(e0, st));
+                    launch_hub(h, c.fp64, g.sm_count, st, vv);
+                    SG_CK(cudaEventRecord(e1, st));
+                    SG_CK(cudaEventSynchronize(e1));
+                    SG_CK(cudaGetLastError());
+                    float t = 0;
+                    cudaEventElapsedTime(&t, e0, e1);
+                    c.launches += 2;
+                    if (t < best) { best = t; variant = vv; }
+                    if (std::getenv("SG_TUNE_LOG"))
+                        std::fprintf(stderr, "[sg tune] hub %s variant %d: %.3f ms\n", key.c_str(), vv, t);
+                }
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                std::lock_guard<std::mutex> lk(g_state_mu);
+                g_hub_tuned[key] = variant;
+            }
+        }
+        // the exact-order hub kernel is latency-bound (long dependent chains): it
+        // runs on the side stream while the tiles without hubs run on st
+        side = h.exact_order && !h.k_leaf;
+        cudaStream_t hs = st;
+        if (side) {
+            GraphState &gs = c.gs;
+            if (!gs.hub_stream) {
+                SG_CK(cudaStreamCreateWithFlags(&gs.hub_stream, cudaStreamNonBlocking));
+                SG_CK(cudaEventCreateWithFlags(&gs.ev_in, cudaEventDisableTiming));
+                SG_CK(cudaEventCreateWithFlags(&gs.ev_hub, cudaEventDisableTiming));
+            }
+            hs = gs.hub_stream;
+            SG_CK(cudaEventRecord(gs.ev_in, st));
+            SG_CK(cudaStreamWaitEvent(hs, gs.ev_in, 0));
+        }
         if (c.profile) {
             SG_CKS(ev_pair(c.hub_ev));
-            SG_CK(cudaEventRecord(c.hub_ev.back().first, st));
+            SG_CK(cudaEventRecord(c.hub_ev.back().first, hs));
         }
-        launch_hub(h, c.fp64, g.sm_count, st);
-        if (c.profile) SG_CK(cudaEventRecord(c.hub_ev.back().second, st));
+        launch_hub(h, c.fp64, g.sm_count, hs, variant);
+        if (c.profile) SG_CK(cudaEventRecord(c.hub_ev.back().second, hs));
+        if (side) SG_CK(cudaEventRecord(c.gs.ev_hub, hs));
         c.launches += 1;
     }
     FusedConfig cfg;
@@ -867,7 +1087,8 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
         // (tile vertices, CTA threads) candidate on the real inputs; all of them
         // compute the same values, so the trial launches only cost time
         const std::string key = graph_sig(g) + shape_key(d, c.fp64, c.hubs.count) + (d.aoff ? "/pk" : "/ex") +
-                                (d.blk ? "/bk" : "") + "/n" + std::to_string(d.nb) + "/l" + std::to_string(c.lay);
+                                (d.blk ? "/bk" : "") + (d.rblk ? "/rt" : "") + "/n" + std::to_string(d.nb) + "/l" +
+                                std::to_string(c.lay);
         TileShape pick{d.tile_v, d.nthreads, d.packed};
         bool have = false;
         {
@@ -876,6 +1097,7 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
             if (it != g_tuned.end()) { pick = it->second; have = true; }
         }
         if (!have && c.autotune) {
+            if (side) SG_CK(cudaStreamWaitEvent(st, c.gs.ev_hub, 0));   // trial launches read the hub rows
             cudaEvent_t e0, e1;
             SG_CK(cudaEventCreate(&e0));
             SG_CK(cudaEventCreate(&e1));
@@ -918,7 +1140,23 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
         SG_CKS(ev_pair(c.fused_ev));
         SG_CK(cudaEventRecord(c.fused_ev.back().first, st));
     }
-    launch_fused(d, c.fp64, cfg, st);
+    if (side) {
+        // tiles without hub vertices first (overlapping the hub kernel), then,
+        // once the hub rows exist, the tiles that hold hubs
+        const int hub_tiles = std::min(d.ntiles, (c.hubs.count + d.tile_v - 1) / d.tile_v);
+        if (hub_tiles < d.ntiles) {
+            StageDesc da = d;
+            da.tile_begin = hub_tiles;
+            launch_fused(da, c.fp64, cfg, st);
+        }
+        SG_CK(cudaStreamWaitEvent(st, c.gs.ev_hub, 0));
+        StageDesc db = d;
+        db.ntiles = hub_tiles;
+        launch_fused(db, c.fp64, cfg, st);
+        c.launches += 1;
+    } else {
+        launch_fused(d, c.fp64, cfg, st);
+    }
     if (c.profile) {
         SG_CK(cudaEventRecord(c.fused_ev.back().second, st));
         // compulsory traffic: main and aux tables read once (a one-hot child is read
@@ -1409,6 +1647,7 @@ Status count_grouped(RunCtx &c, const CountOptions &o, double *raw, CountStats *
     SG_CK(cudaEventRecord(e1, st));
     SG_CK(cudaMemcpyAsync(raw, c.gs.ws.raw, sizeof(double) * o.n_colorings, cudaMemcpyDeviceToHost, st));
     SG_CK(cudaStreamSynchronize(st));
+    SG_CKS(hub_status(c.gs, c.hubs));
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
@@ -1440,10 +1679,15 @@ Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, 
     RunCtx c{g, p, gs, nullptr, o.mode == kModeFP64, (size_t)(o.mode == kModeFP64 ? 8 : 4), 0, {}, 0, 0, o.mode, 0};
     SG_CKS(make_ctx_tables(g, p, gs, c.tab));
     c.exact = o.exact != 0;
-    c.hubs = plan_hubs(g, c.exact ? 0 : o.hub_threshold);
+    // hubs in exact order (the per-tile sums) on the plain and grouped forms;
+    // the persistent queue chunks them (another summation order), or in exact
+    // mode aggregates every vertex in its tile
+    const bool queue = o.batch > 0 && o.persistent && o.mode != kModeOriginal;
+    c.hubs = queue ? plan_hubs(g, c.exact ? 0 : o.hub_threshold, false) : plan_hubs(g, o.hub_threshold, true);
     c.profile = o.profile != 0;
     c.autotune = o.autotune != 0;
     c.blocked = o.blocked != 0;
+    c.rooted = o.rooted != 0;
     // mode 2 carries its aggregation buffer from one coloring to the next, so
     // its colorings always run one after another (the plain form)
     if (o.batch > 0 && o.mode != kModeOriginal)
@@ -1476,6 +1720,7 @@ Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, 
     if (o.mode == kModeOriginal && o.orig_state)
         SG_CK(cudaMemcpyAsync(o.orig_state, gs.ws.orig_buf, 4 * (size_t)g.V, cudaMemcpyDeviceToHost, st));
     SG_CK(cudaStreamSynchronize(st));
+    SG_CKS(hub_status(gs, c.hubs));
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
@@ -1524,9 +1769,10 @@ static Status run_partial(DeviceGraph &g, const Plan &p, uint32_t seed, int mode
 {
     if (g.V >= (1 << 28)) return Status{1, "counting supports graphs of fewer than 2^28 vertices"};
     SG_CKS(make_ctx_tables(g, p, gs, c.tab));
-    // the parity helpers are exact when no hub chunking is asked for
-    c.exact = hub_threshold == 0;
-    c.hubs = plan_hubs(g, hub_threshold);
+    // the parity helpers run the reference's operation order; vertices above
+    // hub_threshold go through the exact-order hub kernel
+    c.exact = true;
+    c.hubs = plan_hubs(g, hub_threshold, true);
     c.use_adjc = adjc_ok(g, p);
     SG_CKS(prepare(c, 1, 1));
     SG_CKS(upload_windows(c, seed, 1));
@@ -1537,7 +1783,7 @@ static Status run_partial(DeviceGraph &g, const Plan &p, uint32_t seed, int mode
         SG_CKS(run_stage(c, 0, s, upto == 0 ? gs.ws.root_vertex : nullptr, g.stream));
     }
     SG_CK(cudaStreamSynchronize(g.stream));
-    return Status::ok();
+    return hub_status(gs, c.hubs);
 }
 
 Status debug_sub_table(DeviceGraph &g, const Plan &p, uint32_t seed, int mode, int hub_threshold, int s, void *out)
@@ -1622,7 +1868,7 @@ Status count_jobs(DeviceGraph &g, const std::vector<const Plan *> &plans, const 
     const int n = (int)plans.size();
     if (n < 1) return Status{1, "no jobs"};
     if (!seeds || !raw) return Status{1, "null argument"};
-    if (o.mode < 0 || o.mode > 2) return Status{1, "unknown count mode"};
+    if (o.mode < 0 || o.mode > 3) return Status{1, "unknown count mode"};
     for (const Plan *p : plans)
         if (!p) return Status{1, "null template plan"};
     if (g.V >= (1 << 28)) return Status{1, "counting supports graphs of fewer than 2^28 vertices"};
@@ -1633,7 +1879,7 @@ Status count_jobs(DeviceGraph &g, const std::vector<const Plan *> &plans, const 
     const size_t es = fp64 ? 8 : 4;
     const size_t V = (size_t)g.V;
     cudaStream_t st = g.stream;
-    const Hubs hubs = plan_hubs(g, o.exact ? 0 : o.hub_threshold);
+    const Hubs hubs = plan_hubs(g, o.exact ? 0 : o.hub_threshold, false);
 
     // one context per job: its plan's device tables, its tables at arena_base
     std::vector<RunCtx> ctx;
@@ -1804,7 +2050,7 @@ Status count_jobs_streams(DeviceGraph &g, const std::vector<const Plan *> &plans
     const int n = (int)plans.size();
     if (n < 1) return Status{1, "no jobs"};
     if (!seeds || !raw) return Status{1, "null argument"};
-    if (o.mode < 0 || o.mode > 2) return Status{1, "unknown count mode"};
+    if (o.mode < 0 || o.mode > 3) return Status{1, "unknown count mode"};
     for (const Plan *p : plans)
         if (!p) return Status{1, "null template plan"};
     if (g.V >= (1 << 28)) return Status{1, "counting supports graphs of fewer than 2^28 vertices"};
@@ -1815,7 +2061,7 @@ Status count_jobs_streams(DeviceGraph &g, const std::vector<const Plan *> &plans
     const size_t es = fp64 ? 8 : 4;
     const size_t V = (size_t)g.V;
     cudaStream_t st = g.stream;
-    const Hubs hubs = plan_hubs(g, o.exact ? 0 : o.hub_threshold);
+    const Hubs hubs = plan_hubs(g, o.hub_threshold, true);
     std::vector<RunCtx> ctx;
     ctx.reserve(n);
     size_t max_arena = 16;
@@ -1828,6 +2074,7 @@ Status count_jobs_streams(DeviceGraph &g, const std::vector<const Plan *> &plans
         c.exact = o.exact != 0;
         c.autotune = o.autotune != 0;
         c.blocked = o.blocked != 0;
+        c.rooted = o.rooted != 0;
         c.use_adjc = adjc_ok(g, p);
         max_arena = std::max(max_arena, (size_t)p.arena_units * V * es);
         hub_pitch = std::max<int32_t>(hub_pitch, (int32_t)round_up(p.k, 8));
@@ -1858,6 +2105,8 @@ Status count_jobs_streams(DeviceGraph &g, const std::vector<const Plan *> &plans
         for (int h = 0; h < hubs.count; ++h) cs[h + 1] = cs[h] + (g.h_degree[h] + hubs.chunk - 1) / hubs.chunk;
         SG_CKS(growT(&w.chunk_start, &w.chunk_start_bytes, 4 * cs.size(), st));
         SG_CK(cudaMemcpyAsync(w.chunk_start, cs.data(), 4 * cs.size(), cudaMemcpyHostToDevice, st));
+        SG_CKS(growT(&w.hub_err, &w.hub_err_bytes, 16, st));
+        SG_CK(cudaMemsetAsync(w.hub_err, 0, 4, st));
         SG_CK(cudaStreamSynchronize(st));   // `cs` is pageable and goes out of scope
     }
     {
@@ -1908,6 +2157,7 @@ Status count_jobs_streams(DeviceGraph &g, const std::vector<const Plan *> &plans
     }
     if (!status.code) SG_CK(cudaMemcpyAsync(raw, w.raw, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
     SG_CK(cudaStreamSynchronize(st));
+    if (!status.code) status = hub_status(gs, hubs);
     double total = 0;
     for (int j = 0; j < n; ++j) {
         float ms = 0;

@@ -102,7 +102,7 @@ template <typename T, int NT, int Q, bool PK>
 __global__ void __launch_bounds__(NT) k_fused(StageDesc d)
 {
     extern __shared__ __align__(32) unsigned char smem_raw[];
-    for (int tile = blockIdx.x; tile < d.ntiles; tile += gridDim.x) fused_tile<T, NT, Q, PK>(d, tile, smem_raw);
+    for (int tile = d.tile_begin + blockIdx.x; tile < d.ntiles; tile += gridDim.x) fused_tile<T, NT, Q, PK>(d, tile, smem_raw);
 }
 
 template <typename T, int NT>
@@ -110,6 +110,47 @@ __global__ void __launch_bounds__(NT) k_hub(HubArgs h)
 {
     __shared__ __align__(32) unsigned char smem_raw[NT * 32];
     for (int item = blockIdx.x; item < h.total_chunks; item += gridDim.x) hub_item<T, NT>(h, item, smem_raw);
+}
+
+// Exact-order hub aggregation (hub_item_exact): one warp per (hub, 32-column
+// group) item, items in hub order (degree-descending: the longest lists
+// first), 8 warps a CTA with a 32 x 32 staging tile each.  The variants differ
+// in the batches of 32 neighbour slices a warp keeps in flight (registers);
+// the autotuner picks one per row width.
+constexpr int kHubWarps = 8;
+int hub_variants() { return 3; }
+
+template <typename T, int NBUF>
+__global__ void __launch_bounds__(32 * kHubWarps) k_hub_exact(HubArgs h)
+{
+    extern __shared__ __align__(32) unsigned char smem_raw[];   // 36 KB (FP32), 68 KB (FP64)
+    constexpr int TILE = 32 * hub_stage_stride<T>();
+    const int warp = threadIdx.x >> 5;
+    T *stage = reinterpret_cast<T *>(smem_raw) + (size_t)warp * TILE;
+    const int items = h.hub_count * ((h.L_a + 31) / 32);
+    for (int item = blockIdx.x * kHubWarps + warp; item < items; item += gridDim.x * kHubWarps)
+        hub_item_exact<T, NBUF>(h, item, stage);
+}
+
+template <typename T>
+static void launch_hub_exact(const HubArgs &h, int sm_count, cudaStream_t st, int variant)
+{
+    const int items = h.hub_count * ((h.L_a + 31) / 32);
+    const size_t smem = (size_t)kHubWarps * 32 * hub_stage_stride<T>() * sizeof(T);
+    auto go = [&](auto kern) {
+        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * kHubWarps, smem) != cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+        const int grid = std::max(1, std::min((items + kHubWarps - 1) / kHubWarps, sm_count * per_sm));
+        kern<<<grid, 32 * kHubWarps, smem, st>>>(h);
+    };
+    switch (variant) {
+    case 1: go(k_hub_exact<T, 2>); break;
+    case 2: go(k_hub_exact<T, 4>); break;
+    default: go(k_hub_exact<T, 3>); break;
+    }
 }
 
 // Threads per vertex (gather_group) and chunks per thread (gather_q) of the
@@ -156,16 +197,29 @@ bool blocked_ok(const StageDesc &d, bool fp64, int tv, int nt)
            d.blk_nblocks > 0 && !d.main_leaf && !d.is_root && !d.scaled;
 }
 
-bool shape_fits(const StageDesc &d, bool fp64, int tv, int nt, int packed, size_t limit, size_t &bytes, int &oc)
+// The stage's block tables in the rooted (rooted = 1) or the plain form.
+static void pick_blocks(StageDesc &d, int rooted)
 {
+    d.rooted = rooted;
+    d.blk = rooted ? d.rblk : d.ublk;
+    d.blk_shape = rooted ? d.rblk_shape : d.ublk_shape;
+    d.blk_nblocks = rooted ? d.rblk_nblocks : d.ublk_nblocks;
+}
+
+bool shape_fits(const StageDesc &d0, bool fp64, int tv, int nt, int packed, size_t limit, size_t &bytes, int &oc,
+                int rooted = 0)
+{
+    if (rooted && (packed != 2 || !d0.rblk || d0.nb != 1 || d0.aux_leaf)) return false;
+    StageDesc d = d0;
+    pick_blocks(d, rooted);
     if (packed == 1 && !packed_ok(d, fp64, tv)) return false;
     if (packed == 2 && !blocked_ok(d, fp64, tv, nt)) return false;
-    const int La_rows = d.aux_leaf ? d.nb * d.k : d.aux_cols;
-    const int Lm_rows = d.main_leaf ? 0 : d.main_cols;
+    const int La_rows = d.aux_leaf ? d.nb * d.k : (rooted ? d.r_La : d.aux_cols);
+    const int Lm_rows = d.main_leaf ? 0 : (rooted ? d.r_Lm : d.main_cols);
     // staged output columns: one coloring's L_s, or the launch's wide columns
     // (nb row pitches) in chunks of a multiple of 4
     const int wide = d.nb == 1 ? d.L_s : d.nb * d.s_cstride;
-    oc = (d.is_root || d.main_leaf) ? 0 : (packed == 2 ? d.L_s : std::min(wide, nt >= 1024 ? 256 : 128));
+    oc = (d.is_root || d.main_leaf) ? 0 : (packed == 2 ? (rooted ? d.r_Ls : d.L_s) : std::min(wide, nt >= 1024 ? 256 : 128));
     bytes = fp64 ? tile_smem_bytes<double>(La_rows, Lm_rows, oc, tv, false, d.nb)
                  : tile_smem_bytes<float>(La_rows, Lm_rows, oc, tv, packed == 1, d.nb);
     if (bytes > limit) return false;
@@ -181,7 +235,8 @@ bool set_shape(StageDesc &d, bool fp64, const TileShape &sh)
 {
     size_t bytes;
     int oc;
-    if (!shape_fits(d, fp64, sh.tile_v, sh.threads, sh.packed, 227 * 1024, bytes, oc)) return false;
+    if (!shape_fits(d, fp64, sh.tile_v, sh.threads, sh.packed, 227 * 1024, bytes, oc, sh.rooted)) return false;
+    pick_blocks(d, sh.rooted);
     d.tile_v = sh.tile_v;
     d.nthreads = sh.threads;
     d.packed = sh.packed;
@@ -203,13 +258,19 @@ std::vector<TileShape> candidate_shapes(const StageDesc &d, bool fp64)
     else if (!d.aux_leaf && d.L_a >= 128)   // wide gathers: more threads per CTA for loads in flight
         all = {{8, 256, 0}, {16, 256, 0}, {32, 256, 0}, {32, 512, 0}, {8, 512, 0}, {16, 512, 0}, {16, 1024, 0}};
     else all = {{8, 256, 0}, {16, 256, 0}, {32, 256, 0}, {32, 512, 0}};
-    if (d.blk_shape > 0)   // register-blocked eMA
+    if (d.ublk_shape > 0)   // register-blocked eMA
         for (TileShape t : {TileShape{32, 256, 2}, TileShape{32, 512, 2}, TileShape{16, 256, 2}, TileShape{16, 512, 2}})
             all.push_back(t);
+    if (d.rblk_shape > 0) {   // register-blocked eMA in the rooted form
+        for (TileShape t : {TileShape{32, 256, 2}, TileShape{32, 512, 2}, TileShape{16, 256, 2}, TileShape{16, 512, 2}}) {
+            t.rooted = 1;
+            all.push_back(t);
+        }
+    }
     for (auto &c : all) {
         size_t bytes;
         int oc;
-        if (!shape_fits(d, fp64, c.tile_v, c.threads, c.packed, 227 * 1024, bytes, oc)) continue;
+        if (!shape_fits(d, fp64, c.tile_v, c.threads, c.packed, 227 * 1024, bytes, oc, c.rooted)) continue;
         out.push_back(c);
         // with chunk masks: also without them (the masks save loads but not the
         // instructions around them)
@@ -245,9 +306,13 @@ bool plan_fused(StageDesc &d, bool fp64, int sm_count, FusedConfig &cfg)
     const size_t limits[3] = {56 * 1024, 113 * 1024, 227 * 1024};
     bool ok = false;
     d.packed = 0;
-    // the register-blocked eMA when the stage has one (its sums are those of the per-output loop)
-    for (TileShape t : {TileShape{32, 256, 2}, TileShape{16, 256, 2}, TileShape{32, 512, 2}, TileShape{16, 512, 2}})
-        if (!ok && d.blk_shape > 0) ok = set_shape(d, fp64, t);
+    // the register-blocked eMA when the stage has one (its sums are those of the
+    // per-output loop), the rooted form first
+    for (int rooted : {1, 0})
+        for (TileShape t : {TileShape{32, 256, 2}, TileShape{16, 256, 2}, TileShape{32, 512, 2}, TileShape{16, 512, 2}}) {
+            t.rooted = rooted;
+            if (!ok && (rooted ? d.rblk_shape : d.ublk_shape) > 0) ok = set_shape(d, fp64, t);
+        }
     if (heavy && !ok) {
         // 32-vertex tiles keep the eMA free of bank conflicts; a wide tile gets 512 threads
         const int pk = packed_ok(d, fp64, 32) ? 1 : 0;
@@ -279,7 +344,7 @@ static void launch_fused_q(const StageDesc &d, const FusedConfig &cfg, cudaStrea
         int per_sm = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, cfg.smem) != cudaSuccess || per_sm < 1)
             per_sm = 1;
-        const int grid = std::max(1, std::min(d.ntiles, cfg.grid * per_sm));
+        const int grid = std::max(1, std::min(d.ntiles - d.tile_begin, cfg.grid * per_sm));
         kern<<<grid, NT, cfg.smem, st>>>(d);
     };
     if (d.packed == 1) {
@@ -315,9 +380,14 @@ void launch_fused(const StageDesc &d, bool fp64, const FusedConfig &cfg, cudaStr
     }
 }
 
-void launch_hub(const HubArgs &h, bool fp64, int sm_count, cudaStream_t st)
+void launch_hub(const HubArgs &h, bool fp64, int sm_count, cudaStream_t st, int variant)
 {
     if (h.hub_count == 0 || h.total_chunks == 0) return;
+    if (h.exact_order && !h.k_leaf) {   // colour counts are exact integers in any order
+        if (fp64) launch_hub_exact<double>(h, sm_count, st, variant);
+        else launch_hub_exact<float>(h, sm_count, st, variant);
+        return;
+    }
     const int grid = std::max(1, std::min(h.total_chunks, sm_count * 8));
     if (fp64) k_hub<double, 256><<<grid, 256, 0, st>>>(h);
     else k_hub<float, 256><<<grid, 256, 0, st>>>(h);

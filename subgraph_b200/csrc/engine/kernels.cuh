@@ -55,13 +55,16 @@ struct TileShape {
     int q = 0;       // 32-byte column chunks per aggregation thread (1, 2, 4); 0: the fewest that keep
                      // nine in ten threads busy
     int nomask = 0;  // 1: read every column chunk (no chunk masks)
+    int rooted = 0;  // register-blocked eMA in the rooted form (StageDesc::rooted)
 };
 // Sets an explicit shape (the autotuner's candidates); false when it does not fit.
 bool set_shape(StageDesc &d, bool fp64, const TileShape &shape);
 // The shapes the autotuner times for a stage.
 std::vector<TileShape> candidate_shapes(const StageDesc &d, bool fp64);
 void launch_fused(const StageDesc &d, bool fp64, const FusedConfig &cfg, cudaStream_t st);
-void launch_hub(const HubArgs &h, bool fp64, int sm_count, cudaStream_t st);
+// variant: the exact-order hub kernel's (threads, ring depth) pair, 0 .. hub_variants()-1
+void launch_hub(const HubArgs &h, bool fp64, int sm_count, cudaStream_t st, int variant = 0);
+int hub_variants();
 
 // K2 with the register-blocked eMA (StageDesc::packed == 2)
 void launch_fused_blk(const StageDesc &d, const FusedConfig &cfg, cudaStream_t st);

@@ -41,6 +41,7 @@ struct StageDesc {
     int32_t gather_group;              // threads per vertex in the aggregation
     int32_t gather_q;                  // 32-byte column chunks per thread (1, 2 or 4)
     int32_t ntiles;
+    int32_t tile_begin;                // a launch covers tiles [tile_begin, ntiles)
     int32_t out_chunk;                 // outputs staged in shared memory per pass
     size_t smem;                       // dynamic shared memory bytes
     // vertices [0, hub_count) are aggregated by the hub kernel in neighbour
@@ -71,6 +72,23 @@ struct StageDesc {
     // neighbour of color c_u only adds to sets containing c_u (its other
     // entries are exact zeros): cmask[c][chunk] has bit c_u set when the
     // 32-byte column chunk holds such a set; other chunks are skipped.
+    // Rooted form (register-blocked eMA, one coloring per launch).  A vertex
+    // of color c has non-zero outputs only for sets holding c, and in those
+    // only the splits whose main set holds c give non-zero products; over the
+    // other k-1 colors they form a stage of shape (|s|-1, |main|-1), whose
+    // index tables are the same for every vertex.  The tile then keeps the
+    // aggregate columns lacking c and the main columns holding c, compacted in
+    // that numbering (agg_chunk, main_full), runs the rooted block tables, and
+    // expands the outputs back to the table's columns (out_rank).  Skipped
+    // products are exact zeros: the sums are those of the full loop.
+    int32_t rooted;
+    int32_t r_Ls, r_La, r_Lm;          // rooted output / aggregate / main columns
+    const uint32_t *agg_chunk;         // [k][aux chunks of 8]: rank of the chunk's first column lacking c
+                                       //   | mask of its columns lacking c << 16
+    const int16_t *main_full;          // [k][r_Lm] table column of each rooted main set
+    const int16_t *out_rank;           // [k][L_s] rooted output of each table column, -1: lacks c
+    const int32_t *ublk, *rblk;        // block tables of the two forms (set_shape picks one into blk)
+    int32_t ublk_shape, ublk_nblocks, rblk_shape, rblk_nblocks;
     const int32_t *adjc;               // [nnz], or null (adj)
     const uint16_t *cmask;             // [k][cmask_stride] (with adjc, non-leaf aux), or null: every chunk read
     int32_t cmask_stride;
@@ -97,6 +115,12 @@ struct HubArgs {
     const int32_t *adj;
     const void *aux;
     void *partial;               // [total_chunks][row_pitch]
+    // exact order: every hub is one chunk (all its neighbours) and its columns
+    // are split among lanes, each lane summing its columns over the whole
+    // neighbour list in order -- the reference's summation order
+    int32_t exact_order;
+    int32_t *err;                // exact order: set when a bounded wait runs out
+    long long wait_cycles;       // exact order: the bound of one wait (clock cycles)
 };
 
 // ---------------------------------------------------------------------------

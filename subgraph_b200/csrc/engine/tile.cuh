@@ -242,8 +242,9 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
     const int TVP = TV + 1;
     const int RS = PK ? kPackedRow : TVP;          // row stride of the aggregate and main rows
     const int nbc = d.nb;                          // colorings of this launch
-    const int La_rows = d.aux_leaf ? nbc * d.k : d.aux_cols;
-    const int Lm_rows = d.main_leaf ? 0 : d.main_cols;
+    const bool rooted = BLK && d.rooted;           // compacted rooted operands (one coloring)
+    const int La_rows = d.aux_leaf ? nbc * d.k : (rooted ? d.r_La : d.aux_cols);
+    const int Lm_rows = d.main_leaf ? 0 : (rooted ? d.r_Lm : d.main_cols);
     T *agg_s = reinterpret_cast<T *>(smem_raw);
     T *main_s = agg_s + (size_t)La_rows * RS;
     T *out_s = main_s + (size_t)Lm_rows * RS;
@@ -400,14 +401,32 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                         }
                     }
                 }
+                if (rooted) {
+                    // only the columns lacking this vertex's color, at their rooted rank
+                    const uint32_t *ach = d.agg_chunk + (size_t)__ldg(d.color + v) * nchunk;
 #pragma unroll
-                for (int r = 0; r < Q; ++r) {
-                    const int q = lane_g + G * r;
-                    if (q < nchunk) {
+                    for (int r = 0; r < Q; ++r) {
+                        const int q = lane_g + G * r;
+                        if (q < nchunk) {
+                            const uint32_t w = __ldg(ach + q);
+                            const uint32_t lack = w >> 16;
+                            const int base = (int)(w & 0xffffu);
 #pragma unroll
-                        for (int i = 0; i < CH; ++i) {
-                            const int c = q * CH + i;
-                            if (c < d.aux_cols) agg_s[c * RS + vi] = CT::get(acc[r], i);
+                            for (int i = 0; i < CH; ++i)
+                                if (lack >> i & 1u)
+                                    agg_s[(base + __popc(lack & ((1u << i) - 1u))) * RS + vi] = CT::get(acc[r], i);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < Q; ++r) {
+                        const int q = lane_g + G * r;
+                        if (q < nchunk) {
+#pragma unroll
+                            for (int i = 0; i < CH; ++i) {
+                                const int c = q * CH + i;
+                                if (c < d.aux_cols) agg_s[c * RS + vi] = CT::get(acc[r], i);
+                            }
                         }
                     }
                 }
@@ -417,9 +436,18 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
     // ---- B: main rows --------------------------------------------------------------
     if (!d.main_leaf) {
         const T *mainp = reinterpret_cast<const T *>(d.main);
-        for (int vi = warp; vi < tv; vi += NW) {
-            const T *row = mainp + (size_t)(v0 + vi) * d.main_pitch;
-            for (int c = lane; c < d.main_cols; c += 32) main_s[c * RS + vi] = ld_tab<COH>(row + c);
+        if (rooted) {
+            // the main columns holding this vertex's color, in rooted order
+            for (int vi = warp; vi < tv; vi += NW) {
+                const T *row = mainp + (size_t)(v0 + vi) * d.main_pitch;
+                const int16_t *mf = d.main_full + (size_t)__ldg(d.color + v0 + vi) * d.r_Lm;
+                for (int c = lane; c < d.r_Lm; c += 32) main_s[c * RS + vi] = ld_tab<COH>(row + __ldg(mf + c));
+            }
+        } else {
+            for (int vi = warp; vi < tv; vi += NW) {
+                const T *row = mainp + (size_t)(v0 + vi) * d.main_pitch;
+                for (int c = lane; c < d.main_cols; c += 32) main_s[c * RS + vi] = ld_tab<COH>(row + c);
+            }
         }
     }
     __syncthreads();
@@ -497,9 +525,23 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
             else blk::ema_blocked(d, agg_s, main_s, out_s, RS, TVP, TV, warp, NW, lane);
             __syncthreads();
             const FastDiv fd = fast_div(W, tv * W);
-            for (int idx = tid; idx < tv * W; idx += NT) {
-                const int vj = fdiv(fd, idx), t = idx - vj * W;
-                outp[(size_t)(v0 + vj) * P + t] = t < d.L_s ? out_s[t * TVP + vj] : T(0);
+            if (rooted) {
+                // rooted outputs back to the table's columns; sets lacking the
+                // vertex's color are exact zeros
+                for (int idx = tid; idx < tv * W; idx += NT) {
+                    const int vj = fdiv(fd, idx), t = idx - vj * W;
+                    T val = T(0);
+                    if (t < d.L_s) {
+                        const int r = __ldg(d.out_rank + (size_t)__ldg(d.color + v0 + vj) * d.L_s + t);
+                        if (r >= 0) val = out_s[r * TVP + vj];
+                    }
+                    outp[(size_t)(v0 + vj) * P + t] = val;
+                }
+            } else {
+                for (int idx = tid; idx < tv * W; idx += NT) {
+                    const int vj = fdiv(fd, idx), t = idx - vj * W;
+                    outp[(size_t)(v0 + vj) * P + t] = t < d.L_s ? out_s[t * TVP + vj] : T(0);
+                }
             }
             __syncthreads();
         }
@@ -659,6 +701,98 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
         }
     }
     __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Exact-order hub aggregation.  item = (hub vertex, group of 32 columns), one
+// warp per item.  The sum of a column over a hub's neighbour list in list
+// order -- the reference's order (CSCGraph.hpp:242-307), so the row equals
+// the per-tile aggregation bit for bit -- is one dependent chain of tens of
+// thousands of adds, so the warp splits the two phases:
+//   loads: the 32-column slices of a batch of 32 neighbours, NCH lanes per
+//          slice (one 32-byte chunk each, so a warp load reads whole lines),
+//          NBUF batches ahead in registers;
+//   adds:  the batch goes through shared memory (row u = neighbour u's
+//          slice), and lane l adds column l of the 32 neighbours in order (one
+//          conflict-free shared load and one add per neighbour).
+// Only __syncwarp is needed (the staging tile is the warp's own).  The result
+// is the hub's single partial row (row v: every hub is one chunk).
+// ---------------------------------------------------------------------------
+// row stride (elements) of a warp's staging tile: a multiple of 16 bytes whose
+// word offset between rows is 4 mod 32, so that both the 16-byte stores and
+// the column reads are free of bank conflicts
+template <typename T> __host__ __device__ constexpr int hub_stage_stride() { return sizeof(T) == 4 ? 36 : 34; }
+
+constexpr int kHubIdAhead = 3;   // batches of neighbour ids loaded ahead of their slice loads
+
+template <typename T, int NBUF>
+__device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, T *stage)
+{
+    using CT = Chunk<T>;
+    using C = typename CT::type;
+    constexpr int SS = hub_stage_stride<T>();
+    constexpr int CH = CT::n;        // columns per 32-byte chunk
+    constexpr int NCH = 32 / CH;     // chunks per 32-column slice = lanes per neighbour
+    constexpr int NPI = 32 / NCH;    // neighbours per warp load
+    const int lane = threadIdx.x & 31;
+    const int ln = lane / NCH, lr = lane % NCH;                // this lane's neighbour and chunk in a load
+    const int ngrp = (h.L_a + 31) / 32;
+    const int v = item / ngrp, grp = item - v * ngrp;
+    const int c0 = grp * 32;                                   // first column of the slice
+    const bool lr_in = lr < (h.aux_pitch - c0) / CH;           // this lane's chunk lies inside the row
+    const int beg = __ldg(h.off + v), deg = __ldg(h.off + v + 1) - beg;
+    const int nbt = (deg + 31) / 32;
+    const C *auxc = reinterpret_cast<const C *>(reinterpret_cast<const T *>(h.aux) + c0) + lr;
+    const int rowc = h.aux_pitch / CH;
+    // neighbour ids: lane l holds the id of neighbour l of a batch (one coalesced
+    // load), kHubIdAhead batches ahead of its slice loads; a load takes the ids
+    // of its neighbours from their lanes by shuffles
+    constexpr int IDA = kHubIdAhead;
+    auto id_at = [&](int b) {
+        const int e = b * 32 + lane;
+        return (b < nbt && e < deg) ? __ldg(h.adj + beg + e) : -1;
+    };
+    auto load = [&](C *dst, int myid) {
+#pragma unroll
+        for (int k = 0; k < NCH; ++k) {
+            const int id = __shfl_sync(0xffffffffu, myid, k * NPI + ln);
+            dst[k] = (id >= 0 && lr_in) ? ld_tab<false>(auxc + (size_t)id * rowc) : CT::zero();
+        }
+    };
+    C buf[NBUF][NCH];
+#pragma unroll
+    for (int j = 0; j < NBUF; ++j) load(buf[j], id_at(j));
+    int idq[IDA];   // idq[i]: this lane's id in batch b + NBUF + i at the start of iteration b
+#pragma unroll
+    for (int i = 0; i < IDA; ++i) idq[i] = id_at(NBUF + i);
+    T acc = T(0);
+    for (int b0 = 0; b0 < nbt; b0 += NBUF) {
+#pragma unroll
+        for (int j = 0; j < NBUF; ++j) {
+            const int b = b0 + j;
+            if (b < nbt) {
+#pragma unroll
+                for (int k = 0; k < NCH; ++k)
+                    *reinterpret_cast<C *>(stage + (size_t)(k * NPI + ln) * SS + lr * CH) = buf[j][k];
+                __syncwarp();
+                const int n = min(32, deg - b * 32);
+                // all 32 shared loads first (independent), then the in-order chain of adds
+                T x[32];
+#pragma unroll
+                for (int u = 0; u < 32; ++u) x[u] = stage[(size_t)u * SS + lane];
+#pragma unroll
+                for (int u = 0; u < 32; ++u)
+                    if (u < n) acc = add_rn(acc, x[u]);
+                __syncwarp();
+                // refill this buffer with batch b + NBUF
+                load(buf[j], idq[0]);
+#pragma unroll
+                for (int i = 0; i < IDA - 1; ++i) idq[i] = idq[i + 1];
+                idq[IDA - 1] = id_at(b + NBUF + IDA);
+            }
+        }
+    }
+    if (c0 + lane < h.L_a) reinterpret_cast<T *>(h.partial)[(size_t)v * h.row_pitch + c0 + lane] = acc;
 }
 
 // ---------------------------------------------------------------------------

@@ -39,6 +39,39 @@ int32_t colex_rank(const int *c, int size)
     return (int32_t)r;
 }
 
+void index_tables(int k, int size, int msz, int &L, int &S, std::vector<int32_t> &comb_to_count,
+                  std::vector<int32_t> &main_split, std::vector<int32_t> &aux_split)
+{
+    L = (int)binom(k, size);
+    comb_to_count.assign(L, 0);
+    S = size > 1 ? (int)binom(size, msz) : 0;
+    main_split.assign((size_t)L * S, 0);
+    aux_split.assign((size_t)L * S, 0);
+    std::vector<int> set(size), sel(msz > 0 ? msz : 1);
+    for (int i = 0; i < size; ++i) set[i] = i;
+    for (int li = 0; li < L; ++li) {
+        comb_to_count[li] = colex_rank(set.data(), size);
+        if (size > 1) {
+            for (int i = 0; i < msz; ++i) sel[i] = i;
+            for (int j = 0; j < S; ++j) {
+                int mc[kMaxColors], ac[kMaxColors], nm = 0, na = 0;
+                for (int q = 0, w = 0; q < size; ++q) {
+                    if (w < msz && sel[w] == q) { mc[nm++] = set[q]; ++w; }
+                    else ac[na++] = set[q];
+                }
+                main_split[(size_t)li * S + j] = colex_rank(mc, nm);
+                aux_split[(size_t)li * S + j] = colex_rank(ac, na);
+                // next lexicographic msz-subset of positions
+                for (int q = msz - 1; q >= 0; --q)
+                    if (sel[q] < size - msz + q) { ++sel[q]; for (int r = q + 1; r < msz; ++r) sel[r] = sel[r - 1] + 1; break; }
+            }
+        }
+        // next lexicographic size-subset of colors
+        for (int q = size - 1; q >= 0; --q)
+            if (set[q] < k - size + q) { ++set[q]; for (int r = q + 1; r < size; ++r) set[r] = set[r - 1] + 1; break; }
+    }
+}
+
 bool Template::from_edges(int n, const std::vector<std::pair<int, int>> &edges, Template &t, std::string &err)
 {
     if (n < 2) { err = "template needs at least 2 vertices"; return false; }
@@ -231,40 +264,10 @@ bool make_plan(const Template &t, Plan &p, std::string &err)
     for (int i = 0; i < ns; ++i)
         if (p.subs[i].main != kDummy) { p.subs[p.subs[i].main].parent = i; p.subs[p.subs[i].aux].parent = i; }
     // ---- index tables
-    const int k = p.k;
     for (int si = 0; si < ns; ++si) {
         SubTemplate &s = p.subs[si];
-        s.L = (int)binom(k, s.size);
-        s.comb_to_count.resize(s.L);
-        int msz = s.size > 1 ? p.subs[s.main].size : 0;
-        int asz = s.size - msz;
-        s.S = s.size > 1 ? (int)binom(s.size, msz) : 0;
-        s.main_split.resize((size_t)s.L * s.S);
-        s.aux_split.resize((size_t)s.L * s.S);
-        std::vector<int> set(s.size), sel(msz);
-        for (int i = 0; i < s.size; ++i) set[i] = i;
-        for (int li = 0; li < s.L; ++li) {
-            s.comb_to_count[li] = colex_rank(set.data(), s.size);
-            if (s.size > 1) {
-                for (int i = 0; i < msz; ++i) sel[i] = i;
-                for (int j = 0; j < s.S; ++j) {
-                    int mc[kMaxColors], ac[kMaxColors], nm = 0, na = 0;
-                    for (int q = 0, w = 0; q < s.size; ++q) {
-                        if (w < msz && sel[w] == q) { mc[nm++] = set[q]; ++w; }
-                        else ac[na++] = set[q];
-                    }
-                    (void)asz;
-                    s.main_split[(size_t)li * s.S + j] = colex_rank(mc, nm);
-                    s.aux_split[(size_t)li * s.S + j] = colex_rank(ac, na);
-                    // next lexicographic msz-subset of positions
-                    for (int q = msz - 1; q >= 0; --q)
-                        if (sel[q] < s.size - msz + q) { ++sel[q]; for (int r = q + 1; r < msz; ++r) sel[r] = sel[r - 1] + 1; break; }
-                }
-            }
-            // next lexicographic size-subset of colors
-            for (int q = s.size - 1; q >= 0; --q)
-                if (set[q] < k - s.size + q) { ++set[q]; for (int r = q + 1; r < s.size; ++r) set[r] = set[r - 1] + 1; break; }
-        }
+        const int msz = s.size > 1 ? p.subs[s.main].size : 0;
+        index_tables(p.k, s.size, msz, s.L, s.S, s.comb_to_count, s.main_split, s.aux_split);
     }
     // ---- processing order (CountMat.cpp:277: s = n-1 .. 0) and the scaled sub
     for (int si = ns - 1; si >= 0; --si)

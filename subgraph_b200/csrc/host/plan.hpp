@@ -50,6 +50,13 @@ struct Plan {
     int nsub() const { return (int)subs.size(); }
 };
 
+// IndexSys tables of a color-set size `size` on k colors with main subsets of
+// msz colors (IndexSys.cpp:169-436): comb_to_count[L] (lex index -> colex
+// column), main_split / aux_split [L][S] (main column and the complement's aux
+// column of the j-th lex msz-subset).
+void index_tables(int k, int size, int msz, int &L, int &S, std::vector<int32_t> &comb_to_count,
+                  std::vector<int32_t> &main_split, std::vector<int32_t> &aux_split);
+
 // DivideTemplates::DivideTp + sort_tps (DivideTemplates.cpp:6-327) and
 // IndexSys::initialization (IndexSys.cpp:9-57, 169-436), then the table plan.
 bool make_plan(const Template &t, Plan &p, std::string &err);

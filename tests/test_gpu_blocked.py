@@ -60,3 +60,25 @@ def test_blocked_in_tuned_fast_path():
     exact = sg.count(g, t, 2, 5, exact=True)
     for a, b in zip(fast, exact):
         assert rel(a, b) <= 1e-6
+
+
+def test_rooted_form_equals_full_form(golden):
+    """The rooted form of the register-blocked eMA (a vertex of color c computes
+    only the sets and splits holding c, over the other k-1 colors) gives the
+    full form's values in exact mode, with and without hub rows (table-level
+    bit-exactness of the rooted form is covered by the golden table tests, whose
+    parity helper takes the rooted form wherever a stage has one)."""
+    rng = random.Random(5)
+    trees = [TEMPLATES["tree12"], TEMPLATES["spider7"], TEMPLATES["tree5"]]
+    trees += [(n, prufer_tree(n, rng)) for n in [rng.randint(5, 12) for _ in range(10)]]
+    for gname in ("rmat10", "rmat12"):
+        _, _, _, col, row = golden.graph(gname)
+        g = sg.DeviceGraph(col, row)
+        for n, edges in trees:
+            t = sg.Graph(n, edges)
+            for hub in (0, 16):
+                a = sg.count(g, t, 2, 17, exact=True, hub_threshold=hub)
+                b = sg.count(g, t, 2, 17, exact=True, hub_threshold=hub, rooted=False)
+                # per-vertex values are identical; only the FP64 sum of tile
+                # partials may differ in order if the two runs tile the root differently
+                assert all(rel(x, y) <= 1e-12 for x, y in zip(a, b)), (gname, n, edges, hub, a, b)
