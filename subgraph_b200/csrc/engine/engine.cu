@@ -105,8 +105,6 @@ struct Workspace {
     size_t adjc_bytes = 0;
     float *orig_buf = nullptr;         // [V] isPruned=0 (CSC) aggregation buffer, internal order
     size_t orig_buf_bytes = 0;
-    int32_t *hub_err = nullptr;        // set by the exact-order hub kernel when a bounded wait runs out
-    size_t hub_err_bytes = 0;
     uint64_t generation = 0;   // bumped whenever a buffer above is re-allocated
 };
 
@@ -154,10 +152,6 @@ void free_batch(BatchPlan &b, cudaStream_t stream)
 
 struct GraphState {
     Workspace ws;
-    // the exact-order hub kernel runs on this stream while the tiles without
-    // hubs run on the caller's (events: stage inputs ready, hub rows ready)
-    cudaStream_t hub_stream = nullptr;
-    cudaEvent_t ev_in = nullptr, ev_hub = nullptr;
     std::map<uint64_t, DevicePlanTables> plans;
     std::map<std::string, BatchPlan> batches; // batch shape -> work queue
     std::vector<cudaStream_t> streams;        // job streams (created on first use)
@@ -580,8 +574,7 @@ DeviceGraph::~DeviceGraph()
         if (it != g_state.end()) {
             Workspace &w = it->second.ws;
             for (void *p : {w.arena, (void *)w.colors, (void *)w.partial, (void *)w.raw, (void *)w.windows, w.hub_partial,
-                            (void *)w.chunk_start, (void *)w.root_vertex, (void *)w.adjc, (void *)w.orig_buf,
-                            (void *)w.hub_err})
+                            (void *)w.chunk_start, (void *)w.root_vertex, (void *)w.adjc, (void *)w.orig_buf})
                 if (p) cudaFreeAsync(p, stream);
             for (auto &kv : it->second.plans) {
                 for (auto *p : kv.second.split) if (p) cudaFreeAsync(p, stream);
@@ -602,12 +595,7 @@ DeviceGraph::~DeviceGraph()
                 cudaStreamSynchronize(js);
                 cudaStreamDestroy(js);
             }
-            if (it->second.hub_stream) {
-                cudaStreamSynchronize(it->second.hub_stream);
-                cudaStreamDestroy(it->second.hub_stream);
-            }
-            if (it->second.ev_in) cudaEventDestroy(it->second.ev_in);
-            if (it->second.ev_hub) cudaEventDestroy(it->second.ev_hub);
+
             g_state.erase(it);
         }
     }
@@ -818,10 +806,6 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
     SG_CKS(growT(&w.windows, &w.windows_bytes, 4 * 31 * (size_t)std::max(ncolorings_total, 1), g.stream));
     if (c.use_adjc) SG_CKS(growT(&w.adjc, &w.adjc_bytes, std::max<size_t>(16, 4 * (size_t)g.nnz), g.stream));
     if (c.mode == kModeOriginal) SG_CKS(growT(&w.orig_buf, &w.orig_buf_bytes, std::max<size_t>(16, 4 * V), g.stream));
-    if (c.hubs.exact_order && c.hubs.count > 0) {
-        SG_CKS(growT(&w.hub_err, &w.hub_err_bytes, 16, g.stream));
-        SG_CK(cudaMemsetAsync(w.hub_err, 0, 4, g.stream));
-    }
     if (c.hubs.count > 0) {
         // a partial row holds the aux columns (or colour counts) of up to c.lay colorings
         int32_t maxp = round_up(c.lay * c.p.k, 8);
@@ -837,17 +821,6 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
         SG_CKS(growT(&w.chunk_start, &w.chunk_start_bytes, 4 * cs.size(), g.stream));
         SG_CK(cudaMemcpyAsync(w.chunk_start, cs.data(), 4 * cs.size(), cudaMemcpyHostToDevice, g.stream));
     }
-    return Status::ok();
-}
-
-// After the stream is synchronised: the exact-order hub kernel's error flag
-// (a bounded wait that ran out) as a status.
-Status hub_status(GraphState &gs, const Hubs &hubs)
-{
-    if (!hubs.exact_order || hubs.count == 0 || !gs.ws.hub_err) return Status::ok();
-    int32_t e = 0;
-    SG_CK(cudaMemcpy(&e, gs.ws.hub_err, 4, cudaMemcpyDeviceToHost));
-    if (e) return Status{4, "exact-order hub aggregation: a bounded wait ran out"};
     return Status::ok();
 }
 
@@ -960,8 +933,6 @@ HubArgs make_hub(RunCtx &c, StageDesc &d, void *partial)
     h.total_chunks = c.hubs.total_chunks;
     h.chunk_start = c.gs.ws.chunk_start;
     h.exact_order = c.hubs.exact_order ? 1 : 0;
-    h.err = c.gs.ws.hub_err;
-    h.wait_cycles = 4000000000LL;   // about 2 s at the maximum SM clock
     h.off = g.d_off;
     h.adj = g.d_adj;
     h.aux = d.aux;
@@ -1015,7 +986,6 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
     if (c.mode == kModeOriginal) return run_stage_original(c, slot, s, root_vertex, st);
     DeviceGraph &g = c.g;
     StageDesc d = make_stage(c, slot, s, root_vertex, b0, nb);
-    bool side = false;   // hub rows come from the side stream (event ev_hub)
     if (c.hubs.count > 0) {
         HubArgs h = make_hub(c, d, c.hub_region ? c.hub_region : c.gs.ws.hub_partial);
         int variant = 0;
@@ -1055,28 +1025,12 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
                 g_hub_tuned[key] = variant;
             }
         }
-        // the exact-order hub kernel is latency-bound (long dependent chains): it
-        // runs on the side stream while the tiles without hubs run on st
-        side = h.exact_order && !h.k_leaf;
-        cudaStream_t hs = st;
-        if (side) {
-            GraphState &gs = c.gs;
-            if (!gs.hub_stream) {
-                SG_CK(cudaStreamCreateWithFlags(&gs.hub_stream, cudaStreamNonBlocking));
-                SG_CK(cudaEventCreateWithFlags(&gs.ev_in, cudaEventDisableTiming));
-                SG_CK(cudaEventCreateWithFlags(&gs.ev_hub, cudaEventDisableTiming));
-            }
-            hs = gs.hub_stream;
-            SG_CK(cudaEventRecord(gs.ev_in, st));
-            SG_CK(cudaStreamWaitEvent(hs, gs.ev_in, 0));
-        }
         if (c.profile) {
             SG_CKS(ev_pair(c.hub_ev));
-            SG_CK(cudaEventRecord(c.hub_ev.back().first, hs));
+            SG_CK(cudaEventRecord(c.hub_ev.back().first, st));
         }
-        launch_hub(h, c.fp64, g.sm_count, hs, variant);
-        if (c.profile) SG_CK(cudaEventRecord(c.hub_ev.back().second, hs));
-        if (side) SG_CK(cudaEventRecord(c.gs.ev_hub, hs));
+        launch_hub(h, c.fp64, g.sm_count, st, variant);
+        if (c.profile) SG_CK(cudaEventRecord(c.hub_ev.back().second, st));
         c.launches += 1;
     }
     FusedConfig cfg;
@@ -1097,7 +1051,6 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
             if (it != g_tuned.end()) { pick = it->second; have = true; }
         }
         if (!have && c.autotune) {
-            if (side) SG_CK(cudaStreamWaitEvent(st, c.gs.ev_hub, 0));   // trial launches read the hub rows
             cudaEvent_t e0, e1;
             SG_CK(cudaEventCreate(&e0));
             SG_CK(cudaEventCreate(&e1));
@@ -1140,23 +1093,7 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
         SG_CKS(ev_pair(c.fused_ev));
         SG_CK(cudaEventRecord(c.fused_ev.back().first, st));
     }
-    if (side) {
-        // tiles without hub vertices first (overlapping the hub kernel), then,
-        // once the hub rows exist, the tiles that hold hubs
-        const int hub_tiles = std::min(d.ntiles, (c.hubs.count + d.tile_v - 1) / d.tile_v);
-        if (hub_tiles < d.ntiles) {
-            StageDesc da = d;
-            da.tile_begin = hub_tiles;
-            launch_fused(da, c.fp64, cfg, st);
-        }
-        SG_CK(cudaStreamWaitEvent(st, c.gs.ev_hub, 0));
-        StageDesc db = d;
-        db.ntiles = hub_tiles;
-        launch_fused(db, c.fp64, cfg, st);
-        c.launches += 1;
-    } else {
-        launch_fused(d, c.fp64, cfg, st);
-    }
+    launch_fused(d, c.fp64, cfg, st);
     if (c.profile) {
         SG_CK(cudaEventRecord(c.fused_ev.back().second, st));
         // compulsory traffic: main and aux tables read once (a one-hot child is read
@@ -1647,7 +1584,6 @@ Status count_grouped(RunCtx &c, const CountOptions &o, double *raw, CountStats *
     SG_CK(cudaEventRecord(e1, st));
     SG_CK(cudaMemcpyAsync(raw, c.gs.ws.raw, sizeof(double) * o.n_colorings, cudaMemcpyDeviceToHost, st));
     SG_CK(cudaStreamSynchronize(st));
-    SG_CKS(hub_status(c.gs, c.hubs));
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
@@ -1720,7 +1656,6 @@ Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, 
     if (o.mode == kModeOriginal && o.orig_state)
         SG_CK(cudaMemcpyAsync(o.orig_state, gs.ws.orig_buf, 4 * (size_t)g.V, cudaMemcpyDeviceToHost, st));
     SG_CK(cudaStreamSynchronize(st));
-    SG_CKS(hub_status(gs, c.hubs));
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
@@ -1783,7 +1718,7 @@ static Status run_partial(DeviceGraph &g, const Plan &p, uint32_t seed, int mode
         SG_CKS(run_stage(c, 0, s, upto == 0 ? gs.ws.root_vertex : nullptr, g.stream));
     }
     SG_CK(cudaStreamSynchronize(g.stream));
-    return hub_status(gs, c.hubs);
+    return Status::ok();
 }
 
 Status debug_sub_table(DeviceGraph &g, const Plan &p, uint32_t seed, int mode, int hub_threshold, int s, void *out)
@@ -2105,8 +2040,6 @@ Status count_jobs_streams(DeviceGraph &g, const std::vector<const Plan *> &plans
         for (int h = 0; h < hubs.count; ++h) cs[h + 1] = cs[h] + (g.h_degree[h] + hubs.chunk - 1) / hubs.chunk;
         SG_CKS(growT(&w.chunk_start, &w.chunk_start_bytes, 4 * cs.size(), st));
         SG_CK(cudaMemcpyAsync(w.chunk_start, cs.data(), 4 * cs.size(), cudaMemcpyHostToDevice, st));
-        SG_CKS(growT(&w.hub_err, &w.hub_err_bytes, 16, st));
-        SG_CK(cudaMemsetAsync(w.hub_err, 0, 4, st));
         SG_CK(cudaStreamSynchronize(st));   // `cs` is pageable and goes out of scope
     }
     {
@@ -2157,7 +2090,6 @@ Status count_jobs_streams(DeviceGraph &g, const std::vector<const Plan *> &plans
     }
     if (!status.code) SG_CK(cudaMemcpyAsync(raw, w.raw, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
     SG_CK(cudaStreamSynchronize(st));
-    if (!status.code) status = hub_status(gs, hubs);
     double total = 0;
     for (int j = 0; j < n; ++j) {
         float ms = 0;

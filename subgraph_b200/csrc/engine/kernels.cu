@@ -114,42 +114,45 @@ __global__ void __launch_bounds__(NT) k_hub(HubArgs h)
 
 // Exact-order hub aggregation (hub_item_exact): one warp per (hub, 32-column
 // group) item, items in hub order (degree-descending: the longest lists
-// first), 8 warps a CTA with a 32 x 32 staging tile each.  The variants differ
-// in the batches of 32 neighbour slices a warp keeps in flight (registers);
-// the autotuner picks one per row width.
-constexpr int kHubWarps = 8;
+// first), W warps a CTA, each with a ring of NSLOT staging tiles.  The
+// variants trade warps per SM against batches in flight per warp; the
+// autotuner picks one per row width.
 int hub_variants() { return 3; }
 
-template <typename T, int NBUF>
-__global__ void __launch_bounds__(32 * kHubWarps) k_hub_exact(HubArgs h)
+template <typename T, int W, int NSLOT>
+__global__ void __launch_bounds__(32 * W) k_hub_exact(HubArgs h)
 {
-    extern __shared__ __align__(32) unsigned char smem_raw[];   // 36 KB (FP32), 68 KB (FP64)
-    constexpr int TILE = 32 * hub_stage_stride<T>();
+    extern __shared__ __align__(32) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5;
-    T *stage = reinterpret_cast<T *>(smem_raw) + (size_t)warp * TILE;
+    T *ring = reinterpret_cast<T *>(smem_raw) + (size_t)warp * NSLOT * hub_tile_elems<T>();
     const int items = h.hub_count * ((h.L_a + 31) / 32);
-    for (int item = blockIdx.x * kHubWarps + warp; item < items; item += gridDim.x * kHubWarps)
-        hub_item_exact<T, NBUF>(h, item, stage);
+    for (int item = blockIdx.x * W + warp; item < items; item += gridDim.x * W)
+        hub_item_exact<T, NSLOT>(h, item, ring);
+}
+
+template <typename T, int W, int NSLOT>
+static void launch_hub_exact_v(const HubArgs &h, int sm_count, cudaStream_t st)
+{
+    const int items = h.hub_count * ((h.L_a + 31) / 32);
+    const size_t smem = (size_t)W * NSLOT * hub_tile_elems<T>() * sizeof(T);
+    auto kern = k_hub_exact<T, W, NSLOT>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * W, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const int grid = std::max(1, std::min((items + W - 1) / W, sm_count * per_sm));
+    kern<<<grid, 32 * W, smem, st>>>(h);
 }
 
 template <typename T>
 static void launch_hub_exact(const HubArgs &h, int sm_count, cudaStream_t st, int variant)
 {
-    const int items = h.hub_count * ((h.L_a + 31) / 32);
-    const size_t smem = (size_t)kHubWarps * 32 * hub_stage_stride<T>() * sizeof(T);
-    auto go = [&](auto kern) {
-        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * kHubWarps, smem) != cudaSuccess ||
-            per_sm < 1)
-            per_sm = 1;
-        const int grid = std::max(1, std::min((items + kHubWarps - 1) / kHubWarps, sm_count * per_sm));
-        kern<<<grid, 32 * kHubWarps, smem, st>>>(h);
-    };
+    // tiles: 4.6 KB (FP32) / 8.7 KB (FP64); every variant stays under 227 KB a CTA
+    constexpr bool D = sizeof(T) == 8;
     switch (variant) {
-    case 1: go(k_hub_exact<T, 2>); break;
-    case 2: go(k_hub_exact<T, 4>); break;
-    default: go(k_hub_exact<T, 3>); break;
+    case 1: launch_hub_exact_v<T, 4, D ? 6 : 6>(h, sm_count, st); break;
+    case 2: launch_hub_exact_v<T, D ? 2 : 4, 12>(h, sm_count, st); break;
+    default: launch_hub_exact_v<T, D ? 4 : 8, D ? 3 : 6>(h, sm_count, st); break;
     }
 }
 

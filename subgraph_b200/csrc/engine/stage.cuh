@@ -119,8 +119,6 @@ struct HubArgs {
     // are split among lanes, each lane summing its columns over the whole
     // neighbour list in order -- the reference's summation order
     int32_t exact_order;
-    int32_t *err;                // exact order: set when a bounded wait runs out
-    long long wait_cycles;       // exact order: the bound of one wait (clock cycles)
 };
 
 // ---------------------------------------------------------------------------

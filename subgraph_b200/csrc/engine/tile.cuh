@@ -708,90 +708,98 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
 // warp per item.  The sum of a column over a hub's neighbour list in list
 // order -- the reference's order (CSCGraph.hpp:242-307), so the row equals
 // the per-tile aggregation bit for bit -- is one dependent chain of tens of
-// thousands of adds, so the warp splits the two phases:
-//   loads: the 32-column slices of a batch of 32 neighbours, NCH lanes per
-//          slice (one 32-byte chunk each, so a warp load reads whole lines),
-//          NBUF batches ahead in registers;
-//   adds:  the batch goes through shared memory (row u = neighbour u's
-//          slice), and lane l adds column l of the 32 neighbours in order (one
-//          conflict-free shared load and one add per neighbour).
-// Only __syncwarp is needed (the staging tile is the warp's own).  The result
-// is the hub's single partial row (row v: every hub is one chunk).
+// thousands of adds, fed by loads whose latency must be hidden:
+//   copies: the 32-column slices of a batch of 32 neighbours go straight into
+//           a shared-memory tile (row u = neighbour u's slice) with cp.async,
+//           NCH lanes per slice (one 32-byte chunk each, so a warp's copies
+//           read whole lines), NSLOT batches ahead (a ring of tiles per warp);
+//   adds:   lane l reads column l of the 32 rows (conflict-free shared loads,
+//           all issued first) and adds them in order.
+// Neighbour ids are loaded one per lane per batch, kHubIdAhead batches ahead,
+// and reach the lanes that copy for them by shuffles.  A lane waits for its
+// own copies (cp.async.wait_group) and __syncwarp makes the whole tile
+// visible; the ring belongs to the warp, so nothing wider is synchronised.
+// The result is the hub's single partial row (row v: every hub is one chunk).
 // ---------------------------------------------------------------------------
-// row stride (elements) of a warp's staging tile: a multiple of 16 bytes whose
-// word offset between rows is 4 mod 32, so that both the 16-byte stores and
-// the column reads are free of bank conflicts
+// row stride (elements) of a staging tile: a multiple of 16 bytes whose word
+// offset between rows is 4 mod 32, so that both the 16-byte copies (eight
+// lanes a phase) and the column reads are free of bank conflicts
 template <typename T> __host__ __device__ constexpr int hub_stage_stride() { return sizeof(T) == 4 ? 36 : 34; }
+template <typename T> __host__ __device__ constexpr int hub_tile_elems() { return 32 * hub_stage_stride<T>(); }
 
-constexpr int kHubIdAhead = 3;   // batches of neighbour ids loaded ahead of their slice loads
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-template <typename T, int NBUF>
-__device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, T *stage)
+constexpr int kHubIdAhead = 2;   // batches of neighbour ids loaded ahead of their copies
+
+template <typename T, int NSLOT>
+__device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, T *ring)
 {
     using CT = Chunk<T>;
-    using C = typename CT::type;
     constexpr int SS = hub_stage_stride<T>();
+    constexpr int TILE = hub_tile_elems<T>();
     constexpr int CH = CT::n;        // columns per 32-byte chunk
     constexpr int NCH = 32 / CH;     // chunks per 32-column slice = lanes per neighbour
-    constexpr int NPI = 32 / NCH;    // neighbours per warp load
+    constexpr int NPI = 32 / NCH;    // neighbours per warp copy
+    constexpr int IDA = kHubIdAhead;
     const int lane = threadIdx.x & 31;
-    const int ln = lane / NCH, lr = lane % NCH;                // this lane's neighbour and chunk in a load
+    const int ln = lane / NCH, lr = lane % NCH;                // this lane's neighbour and chunk in a copy
     const int ngrp = (h.L_a + 31) / 32;
     const int v = item / ngrp, grp = item - v * ngrp;
     const int c0 = grp * 32;                                   // first column of the slice
     const bool lr_in = lr < (h.aux_pitch - c0) / CH;           // this lane's chunk lies inside the row
     const int beg = __ldg(h.off + v), deg = __ldg(h.off + v + 1) - beg;
     const int nbt = (deg + 31) / 32;
-    const C *auxc = reinterpret_cast<const C *>(reinterpret_cast<const T *>(h.aux) + c0) + lr;
-    const int rowc = h.aux_pitch / CH;
-    // neighbour ids: lane l holds the id of neighbour l of a batch (one coalesced
-    // load), kHubIdAhead batches ahead of its slice loads; a load takes the ids
-    // of its neighbours from their lanes by shuffles
-    constexpr int IDA = kHubIdAhead;
+    const char *src0 = reinterpret_cast<const char *>(reinterpret_cast<const T *>(h.aux) + c0) + lr * 32;
+    const size_t row_bytes = (size_t)h.aux_pitch * sizeof(T);
     auto id_at = [&](int b) {
         const int e = b * 32 + lane;
         return (b < nbt && e < deg) ? __ldg(h.adj + beg + e) : -1;
     };
-    auto load = [&](C *dst, int myid) {
+    // batch b's copies into ring slot b % NSLOT (rows of neighbours past the
+    // list and chunks past the row are not copied: they are never added)
+    auto issue = [&](int b, int myid) {
+        T *tile = ring + (size_t)(b % NSLOT) * TILE;
 #pragma unroll
         for (int k = 0; k < NCH; ++k) {
             const int id = __shfl_sync(0xffffffffu, myid, k * NPI + ln);
-            dst[k] = (id >= 0 && lr_in) ? ld_tab<false>(auxc + (size_t)id * rowc) : CT::zero();
-        }
-    };
-    C buf[NBUF][NCH];
-#pragma unroll
-    for (int j = 0; j < NBUF; ++j) load(buf[j], id_at(j));
-    int idq[IDA];   // idq[i]: this lane's id in batch b + NBUF + i at the start of iteration b
-#pragma unroll
-    for (int i = 0; i < IDA; ++i) idq[i] = id_at(NBUF + i);
-    T acc = T(0);
-    for (int b0 = 0; b0 < nbt; b0 += NBUF) {
-#pragma unroll
-        for (int j = 0; j < NBUF; ++j) {
-            const int b = b0 + j;
-            if (b < nbt) {
-#pragma unroll
-                for (int k = 0; k < NCH; ++k)
-                    *reinterpret_cast<C *>(stage + (size_t)(k * NPI + ln) * SS + lr * CH) = buf[j][k];
-                __syncwarp();
-                const int n = min(32, deg - b * 32);
-                // all 32 shared loads first (independent), then the in-order chain of adds
-                T x[32];
-#pragma unroll
-                for (int u = 0; u < 32; ++u) x[u] = stage[(size_t)u * SS + lane];
-#pragma unroll
-                for (int u = 0; u < 32; ++u)
-                    if (u < n) acc = add_rn(acc, x[u]);
-                __syncwarp();
-                // refill this buffer with batch b + NBUF
-                load(buf[j], idq[0]);
-#pragma unroll
-                for (int i = 0; i < IDA - 1; ++i) idq[i] = idq[i + 1];
-                idq[IDA - 1] = id_at(b + NBUF + IDA);
+            if (id >= 0 && lr_in) {
+                const char *src = src0 + (size_t)id * row_bytes;
+                char *dst = reinterpret_cast<char *>(tile + (size_t)(k * NPI + ln) * SS + lr * CH);
+                cp_async16(dst, src);
+                cp_async16(dst + 16, src + 16);
             }
         }
+        cp_async_commit();   // always, so that the group count stays in step
+    };
+    int idq[IDA];   // idq[i]: this lane's id in batch b + NSLOT - 1 + i at the start of iteration b
+#pragma unroll
+    for (int i = 0; i < IDA; ++i) idq[i] = id_at(NSLOT - 1 + i);
+    for (int b = 0; b < NSLOT - 1; ++b) issue(b, id_at(b));
+    T acc = T(0);
+    for (int b = 0; b < nbt; ++b) {
+        issue(b + NSLOT - 1, idq[0]);
+#pragma unroll
+        for (int i = 0; i < IDA - 1; ++i) idq[i] = idq[i + 1];
+        idq[IDA - 1] = id_at(b + NSLOT - 1 + IDA);
+        cp_async_wait<NSLOT - 1>();   // this lane's copies of batch b have landed
+        __syncwarp();                 // and so have the other lanes'
+        const T *tile = ring + (size_t)(b % NSLOT) * TILE;
+        const int n = min(32, deg - b * 32);
+        T x[32];
+#pragma unroll
+        for (int u = 0; u < 32; ++u) x[u] = tile[(size_t)u * SS + lane];
+#pragma unroll
+        for (int u = 0; u < 32; ++u)
+            if (u < n) acc = add_rn(acc, x[u]);
+        __syncwarp();                 // the slot is refilled by the next iteration's copies
     }
+    cp_async_wait<0>();
     if (c0 + lane < h.L_a) reinterpret_cast<T *>(h.partial)[(size_t)v * h.row_pitch + c0 + lane] = acc;
 }
 
