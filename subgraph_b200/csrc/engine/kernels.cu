@@ -117,24 +117,25 @@ __global__ void __launch_bounds__(NT) k_hub(HubArgs h)
 // first), W warps a CTA, each with a ring of NSLOT staging tiles.  The
 // variants trade warps per SM against batches in flight per warp; the
 // autotuner picks one per row width.
-int hub_variants() { return 3; }
+int hub_variants() { return 4; }
 
 template <typename T, int W, int NSLOT>
 __global__ void __launch_bounds__(32 * W) k_hub_exact(HubArgs h)
 {
     extern __shared__ __align__(32) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5;
-    T *ring = reinterpret_cast<T *>(smem_raw) + (size_t)warp * NSLOT * hub_tile_elems<T>();
+    unsigned char *wsmem = smem_raw + (size_t)warp * hub_warp_bytes<T, NSLOT>();
     const int items = h.hub_count * ((h.L_a + 31) / 32);
     for (int item = blockIdx.x * W + warp; item < items; item += gridDim.x * W)
-        hub_item_exact<T, NSLOT>(h, item, ring);
+        hub_item_exact<T, NSLOT>(h, item, wsmem);
 }
 
 template <typename T, int W, int NSLOT>
 static void launch_hub_exact_v(const HubArgs &h, int sm_count, cudaStream_t st)
 {
     const int items = h.hub_count * ((h.L_a + 31) / 32);
-    const size_t smem = (size_t)W * NSLOT * hub_tile_elems<T>() * sizeof(T);
+    constexpr size_t smem = (size_t)W * hub_warp_bytes<T, NSLOT>();
+    static_assert(smem <= 227 * 1024, "a CTA's rings must fit shared memory");
     auto kern = k_hub_exact<T, W, NSLOT>;
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
@@ -147,11 +148,14 @@ static void launch_hub_exact_v(const HubArgs &h, int sm_count, cudaStream_t st)
 template <typename T>
 static void launch_hub_exact(const HubArgs &h, int sm_count, cudaStream_t st, int variant)
 {
-    // tiles: 4.6 KB (FP32) / 8.7 KB (FP64); every variant stays under 227 KB a CTA
+    // (warps, ring depth): tiles are 4.6 KB (FP32) / 8.7 KB (FP64), and every
+    // variant stays under 227 KB a CTA; the deep rings serve stages whose few
+    // long hub lists are latency-bound, the many-warp ones wide stages
     constexpr bool D = sizeof(T) == 8;
     switch (variant) {
-    case 1: launch_hub_exact_v<T, 4, D ? 6 : 6>(h, sm_count, st); break;
+    case 1: launch_hub_exact_v<T, 4, 6>(h, sm_count, st); break;
     case 2: launch_hub_exact_v<T, D ? 2 : 4, 12>(h, sm_count, st); break;
+    case 3: launch_hub_exact_v<T, D ? 1 : 2, 24>(h, sm_count, st); break;
     default: launch_hub_exact_v<T, D ? 4 : 8, D ? 3 : 6>(h, sm_count, st); break;
     }
 }

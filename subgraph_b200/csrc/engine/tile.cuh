@@ -711,94 +711,203 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
 // thousands of adds, fed by loads whose latency must be hidden:
 //   copies: the 32-column slices of a batch of 32 neighbours go straight into
 //           a shared-memory tile (row u = neighbour u's slice) with cp.async,
-//           NCH lanes per slice (one 32-byte chunk each, so a warp's copies
-//           read whole lines), NSLOT batches ahead (a ring of tiles per warp);
-//   adds:   lane l reads column l of the 32 rows (conflict-free shared loads,
-//           all issued first) and adds them in order.
-// Neighbour ids are loaded one per lane per batch, kHubIdAhead batches ahead,
-// and reach the lanes that copy for them by shuffles.  A lane waits for its
-// own copies (cp.async.wait_group) and __syncwarp makes the whole tile
-// visible; the ring belongs to the warp, so nothing wider is synchronised.
-// The result is the hub's single partial row (row v: every hub is one chunk).
+//           16 bytes a lane, a copy instruction moving whole slices (full
+//           sectors), NSLOT batches ahead (a ring of tiles per warp);
+//   adds:   lane l reads column l of the 32 rows (conflict-free shared loads)
+//           one batch ahead and adds them in order.
+// Neighbour ids travel through the same pipeline: lane l copies id l of a
+// batch (cp.async, 4 bytes) into a ring of NSLOT + 1 id slots, in the commit
+// group of the rows of the batch NSLOT earlier, so no step waits on a global
+// load: every wait is cp.async.wait_group for a group issued NSLOT - 2
+// batches earlier.  A lane waits for its own copies and __syncwarp makes the
+// whole tile (and id slot) visible; the rings belong to the warp, so nothing
+// wider is synchronised.  The result is the hub's single partial row (row v:
+// every hub is one chunk).
 // ---------------------------------------------------------------------------
 // row stride (elements) of a staging tile: a multiple of 16 bytes whose word
-// offset between rows is 4 mod 32, so that both the 16-byte copies (eight
-// lanes a phase) and the column reads are free of bank conflicts
+// offset between rows is 4 mod 32, so that the column reads are free of bank
+// conflicts (a copy phase of eight lanes writes 128 contiguous bytes)
 template <typename T> __host__ __device__ constexpr int hub_stage_stride() { return sizeof(T) == 4 ? 36 : 34; }
 template <typename T> __host__ __device__ constexpr int hub_tile_elems() { return 32 * hub_stage_stride<T>(); }
+// id slots of a warp's ring (one batch of 32 ids each)
+template <int NSLOT> __host__ __device__ constexpr int hub_id_slots() { return NSLOT + 1; }
+// shared-memory bytes of one warp: the tile ring and the id ring
+template <typename T, int NSLOT> __host__ __device__ constexpr size_t hub_warp_bytes()
+{
+    return (size_t)NSLOT * hub_tile_elems<T>() * sizeof(T) + (size_t)hub_id_slots<NSLOT>() * 32 * sizeof(int32_t);
+}
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
 {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(gmem) : "memory");
+}
+// the same with the shared-memory address given as a 32-bit shared-window offset
+__device__ __forceinline__ void cp_async16_s(uint32_t sa, const void *gmem)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4_s(uint32_t sa, const void *gmem)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(gmem) : "memory");
+}
+// copies of `n` source bytes (n <= the copy size) whose remaining bytes are
+// zero-filled: n = 0 writes zeros and reads nothing
+__device__ __forceinline__ void cp_async16_zs(uint32_t sa, const void *gmem, uint32_t n)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async4_zs(uint32_t sa, const void *gmem, uint32_t n)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(sa), "l"(gmem), "r"(n) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-constexpr int kHubIdAhead = 2;   // batches of neighbour ids loaded ahead of their copies
-
 template <typename T, int NSLOT>
-__device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, T *ring)
+__device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, unsigned char *wsmem)
 {
-    using CT = Chunk<T>;
+    static_assert(NSLOT >= 3, "one batch in flight besides the two in registers");
     constexpr int SS = hub_stage_stride<T>();
     constexpr int TILE = hub_tile_elems<T>();
-    constexpr int CH = CT::n;        // columns per 32-byte chunk
-    constexpr int NCH = 32 / CH;     // chunks per 32-column slice = lanes per neighbour
-    constexpr int NPI = 32 / NCH;    // neighbours per warp copy
-    constexpr int IDA = kHubIdAhead;
+    constexpr int PC = 16 / sizeof(T);   // columns per 16-byte piece
+    constexpr int NP = 32 / PC;          // pieces per 32-column slice = lanes per neighbour of one copy
+    constexpr int NPI = 32 / NP;         // neighbours per warp copy (whole 128-/256-byte slices)
+    constexpr int RPL = 32 / NPI;        // rows per lane group = copies per batch
+    constexpr int IDR = hub_id_slots<NSLOT>();
+    constexpr uint32_t TILE_B = TILE * sizeof(T), IDS_B = 32 * sizeof(int32_t);
+    const T *ring = reinterpret_cast<const T *>(wsmem);
+    const int32_t *ids = reinterpret_cast<const int32_t *>(wsmem + (size_t)NSLOT * TILE_B);
+    const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(wsmem);
+    const uint32_t ids_s = ring_s + NSLOT * TILE_B;
     const int lane = threadIdx.x & 31;
-    const int ln = lane / NCH, lr = lane % NCH;                // this lane's neighbour and chunk in a copy
+    // lane group ln copies piece lr of rows ln * RPL .. ln * RPL + RPL - 1, one
+    // row a copy: each copy instruction moves NPI whole slices (full sectors)
+    const int ln = lane / NP, lr = lane % NP;
     const int ngrp = (h.L_a + 31) / 32;
     const int v = item / ngrp, grp = item - v * ngrp;
     const int c0 = grp * 32;                                   // first column of the slice
-    const bool lr_in = lr < (h.aux_pitch - c0) / CH;           // this lane's chunk lies inside the row
+    const bool lr_in = c0 + (lr + 1) * PC <= h.aux_pitch;      // this lane's piece lies inside the row
     const int beg = __ldg(h.off + v), deg = __ldg(h.off + v + 1) - beg;
     const int nbt = (deg + 31) / 32;
-    const char *src0 = reinterpret_cast<const char *>(reinterpret_cast<const T *>(h.aux) + c0) + lr * 32;
-    const size_t row_bytes = (size_t)h.aux_pitch * sizeof(T);
-    auto id_at = [&](int b) {
-        const int e = b * 32 + lane;
-        return (b < nbt && e < deg) ? __ldg(h.adj + beg + e) : -1;
+    // this lane's piece of row 0 (a lane whose piece lies past the row copies
+    // the slice's first piece instead: columns past the row are never
+    // written out), and its first tile row in slot 0
+    const uint64_t src0 = reinterpret_cast<uint64_t>(reinterpret_cast<const T *>(h.aux) + c0 + (lr_in ? lr * PC : 0));
+    const uint32_t row_bytes = (uint32_t)h.aux_pitch * (uint32_t)sizeof(T);
+    const uint32_t dst0 = ring_s + (uint32_t)((ln * RPL * SS + lr * PC) * sizeof(T));
+    const int32_t *adj_v = h.adj + beg;
+    // id `lane` of batch j into the id slot at byte offset `slot_b` (zero past
+    // the list: a valid row that is never added)
+    auto fetch_ids = [&](int j, uint32_t slot_b) {
+        const int e = j * 32 + lane;
+        const bool in = e < deg;
+        cp_async4_zs(ids_s + slot_b + lane * 4, adj_v + (in ? e : 0), in ? 4u : 0u);
     };
-    // batch b's copies into ring slot b % NSLOT (rows of neighbours past the
-    // list and chunks past the row are not copied: they are never added)
-    auto issue = [&](int b, int myid) {
-        T *tile = ring + (size_t)(b % NSLOT) * TILE;
+    // A batch's copy plan for this lane: the source of each of its RPL pieces.
+    uint64_t src[RPL];
+    auto plan = [&](uint32_t is_b) {
+        const int4 *bid = reinterpret_cast<const int4 *>(ids + is_b / 4 + ln * RPL);
 #pragma unroll
-        for (int k = 0; k < NCH; ++k) {
-            const int id = __shfl_sync(0xffffffffu, myid, k * NPI + ln);
-            if (id >= 0 && lr_in) {
-                const char *src = src0 + (size_t)id * row_bytes;
-                char *dst = reinterpret_cast<char *>(tile + (size_t)(k * NPI + ln) * SS + lr * CH);
-                cp_async16(dst, src);
-                cp_async16(dst + 16, src + 16);
-            }
+        for (int q = 0; q < RPL / 4; ++q) {
+            const int4 t = bid[q];
+            src[4 * q] = src0 + (uint64_t)(uint32_t)t.x * row_bytes;
+            src[4 * q + 1] = src0 + (uint64_t)(uint32_t)t.y * row_bytes;
+            src[4 * q + 2] = src0 + (uint64_t)(uint32_t)t.z * row_bytes;
+            src[4 * q + 3] = src0 + (uint64_t)(uint32_t)t.w * row_bytes;
         }
-        cp_async_commit();   // always, so that the group count stays in step
     };
-    int idq[IDA];   // idq[i]: this lane's id in batch b + NSLOT - 1 + i at the start of iteration b
+    // batch b's copies into the ring slot at byte offset ts_b: every row of a
+    // full batch, the rows inside the list of the last one, none past it
+    auto copy = [&](int b, uint32_t ts_b) {
+        const int left = deg - b * 32;
+        const uint32_t d = dst0 + ts_b;
+        if (left >= 32) {
 #pragma unroll
-    for (int i = 0; i < IDA; ++i) idq[i] = id_at(NSLOT - 1 + i);
-    for (int b = 0; b < NSLOT - 1; ++b) issue(b, id_at(b));
-    T acc = T(0);
-    for (int b = 0; b < nbt; ++b) {
-        issue(b + NSLOT - 1, idq[0]);
+            for (int k = 0; k < RPL; ++k) cp_async16_s(d + (uint32_t)(k * SS * sizeof(T)), reinterpret_cast<const void *>(src[k]));
+        } else if (left > 0) {
 #pragma unroll
-        for (int i = 0; i < IDA - 1; ++i) idq[i] = idq[i + 1];
-        idq[IDA - 1] = id_at(b + NSLOT - 1 + IDA);
-        cp_async_wait<NSLOT - 1>();   // this lane's copies of batch b have landed
-        __syncwarp();                 // and so have the other lanes'
-        const T *tile = ring + (size_t)(b % NSLOT) * TILE;
-        const int n = min(32, deg - b * 32);
-        T x[32];
+            for (int k = 0; k < RPL; ++k)
+                if (ln * RPL + k < left)
+                    cp_async16_s(d + (uint32_t)(k * SS * sizeof(T)), reinterpret_cast<const void *>(src[k]));
+        }
+    };
+    auto load = [&](T(&x)[32], uint32_t ts_b) {
+        const T *tile = ring + ts_b / sizeof(T) + lane;
 #pragma unroll
-        for (int u = 0; u < 32; ++u) x[u] = tile[(size_t)u * SS + lane];
-#pragma unroll
-        for (int u = 0; u < 32; ++u)
-            if (u < n) acc = add_rn(acc, x[u]);
-        __syncwarp();                 // the slot is refilled by the next iteration's copies
+        for (int u = 0; u < 32; ++u) x[u] = tile[u * SS];
+    };
+    // ids of batches 0 .. NSLOT - 1 first; batch j >= NSLOT has its ids
+    // fetched with batch j - NSLOT's rows, into the slot of batch j - NSLOT - 1
+    // (whose ids the previous plan read: hence the __syncwarp)
+    for (int j = 0; j < NSLOT; ++j) fetch_ids(j, j * IDS_B);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncwarp();
+    for (int b = 0; b < NSLOT - 1; ++b) {
+        plan(b * IDS_B);
+        copy(b, b * TILE_B);
+        __syncwarp();
+        fetch_ids(b + NSLOT, (b == 0 ? IDR - 1 : b - 1) * IDS_B);
+        cp_async_commit();
     }
+    plan((NSLOT - 1) * IDS_B);
+    // Step b: copy batch b + NSLOT - 1 (planned by the step before) and fetch
+    // the ids of batch b + 2 NSLOT - 1; wait for batch b + 1 and read it into
+    // registers; plan batch b + NSLOT; add batch b (read by the step before).
+    // Steps b < nbt - NSLOT copy and add full batches and have no branch, so
+    // that the copies, the shared loads and the plan fill the latency of the
+    // add chains; the last NSLOT steps copy what is left of the list and add
+    // the last batch under a predicate.  Slots (byte offsets) advance by one.
+    uint32_t ts_b = (NSLOT - 1) * TILE_B, is_b = (NSLOT - 1) * IDS_B, ls_b = TILE_B;
+    T acc = T(0);
+    auto step = [&](int b, T(&cur)[32], T(&nxt)[32], bool tail, bool last) {
+        if (!tail) {
+#pragma unroll
+            for (int k = 0; k < RPL; ++k)
+                cp_async16_s(dst0 + ts_b + (uint32_t)(k * SS * sizeof(T)), reinterpret_cast<const void *>(src[k]));
+        } else {
+            copy(b + NSLOT - 1, ts_b);
+        }
+        fetch_ids(b + 2 * NSLOT - 1, is_b == 0 ? (IDR - 1) * IDS_B : is_b - IDS_B);
+        cp_async_commit();            // always, so that the group count stays in step
+        ts_b = ts_b == (NSLOT - 1) * TILE_B ? 0 : ts_b + TILE_B;
+        is_b = is_b == (IDR - 1) * IDS_B ? 0 : is_b + IDS_B;
+        cp_async_wait<NSLOT - 2>();   // this lane's copies of batch b + 1 (and older) have landed
+        __syncwarp();                 // and so have the other lanes'; the slots read two steps ago may be refilled
+        load(nxt, ls_b);              // batch b + 1 (unused past the list)
+        ls_b = ls_b == (NSLOT - 1) * TILE_B ? 0 : ls_b + TILE_B;
+        plan(is_b);                   // batch b + NSLOT: its ids landed with batch b's rows
+        if (!last) {
+#pragma unroll
+            for (int u = 0; u < 32; ++u) acc = add_rn(acc, cur[u]);
+        } else {
+            const int n = deg - b * 32;
+#pragma unroll
+            for (int u = 0; u < 32; ++u)
+                if (u < n) acc = add_rn(acc, cur[u]);
+        }
+    };
+    T x[32], y[32];
+    cp_async_wait<NSLOT - 2>();   // batch 0
+    __syncwarp();
+    load(x, 0);
+    const int main_end = nbt - NSLOT;
+    int b = 0;
+    for (; b + 1 < main_end; b += 2) {
+        step(b, x, y, false, false);
+        step(b + 1, y, x, false, false);
+    }
+    for (; b + 1 < nbt; b += 2) {
+        step(b, x, y, true, false);
+        step(b + 1, y, x, true, b + 2 == nbt);
+    }
+    if (b < nbt) step(b, x, y, true, true);
     cp_async_wait<0>();
     if (c0 + lane < h.L_a) reinterpret_cast<T *>(h.partial)[(size_t)v * h.row_pitch + c0 + lane] = acc;
 }
