@@ -160,10 +160,12 @@ typedef struct {
     int32_t no_autotune;    /* != 0: use the default tile shapes instead of timing the
                                candidates of each new stage shape once per graph */
     int32_t exact;          /* != 0: the reference's FP32 operations in the reference's
-                               order for every vertex and product (no hub chunking, no
-                               fused multiply-add): per-vertex values bit-identical to
-                               the reference; otherwise products may be fused (one
-                               rounding) and hub neighbour lists summed in chunks */
+                               order for every vertex and product (no fused multiply-add,
+                               no hub chunking): per-vertex values bit-identical to the
+                               reference; otherwise products may be fused (one rounding).
+                               Hub neighbour lists are summed in the reference's order in
+                               the plain and grouped forms either way; the persistent form
+                               sums them in chunks unless exact is set */
     int32_t wait_limit_ms;  /* batched form: how long a work item may wait for its inputs
                                before the call fails with SG_ERR_TIMEOUT (0 = 2000 ms) */
     int32_t no_blocked;     /* 1: no register-blocked eMA (every output computed by its
