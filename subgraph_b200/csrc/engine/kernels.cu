@@ -117,26 +117,26 @@ __global__ void __launch_bounds__(NT) k_hub(HubArgs h)
 // first), W warps a CTA, each with a ring of NSLOT staging tiles.  The
 // variants trade warps per SM against batches in flight per warp; the
 // autotuner picks one per row width.
-int hub_variants() { return 4; }
+int hub_variants() { return 6; }
 
-template <typename T, int W, int NSLOT>
+template <typename T, int W, int NSLOT, int BR>
 __global__ void __launch_bounds__(32 * W) k_hub_exact(HubArgs h)
 {
     extern __shared__ __align__(32) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5;
-    unsigned char *wsmem = smem_raw + (size_t)warp * hub_warp_bytes<T, NSLOT>();
+    unsigned char *wsmem = smem_raw + (size_t)warp * hub_warp_bytes<T, NSLOT, BR>();
     const int items = h.hub_count * ((h.L_a + 31) / 32);
     for (int item = blockIdx.x * W + warp; item < items; item += gridDim.x * W)
-        hub_item_exact<T, NSLOT>(h, item, wsmem);
+        hub_item_exact<T, NSLOT, BR>(h, item, wsmem);
 }
 
-template <typename T, int W, int NSLOT>
+template <typename T, int W, int NSLOT, int BR = 32>
 static void launch_hub_exact_v(const HubArgs &h, int sm_count, cudaStream_t st)
 {
     const int items = h.hub_count * ((h.L_a + 31) / 32);
-    constexpr size_t smem = (size_t)W * hub_warp_bytes<T, NSLOT>();
+    constexpr size_t smem = (size_t)W * hub_warp_bytes<T, NSLOT, BR>();
     static_assert(smem <= 227 * 1024, "a CTA's rings must fit shared memory");
-    auto kern = k_hub_exact<T, W, NSLOT>;
+    auto kern = k_hub_exact<T, W, NSLOT, BR>;
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * W, smem) != cudaSuccess || per_sm < 1)
@@ -148,14 +148,24 @@ static void launch_hub_exact_v(const HubArgs &h, int sm_count, cudaStream_t st)
 template <typename T>
 static void launch_hub_exact(const HubArgs &h, int sm_count, cudaStream_t st, int variant)
 {
-    // (warps, ring depth): tiles are 4.6 KB (FP32) / 8.7 KB (FP64), and every
-    // variant stays under 227 KB a CTA; the deep rings serve stages whose few
-    // long hub lists are latency-bound, the many-warp ones wide stages
+    // (warps, ring depth, batch rows): 32-row tiles are 4.6 KB (FP32) / 8.7 KB
+    // (FP64), and every variant stays under 227 KB a CTA; the deep rings serve
+    // stages whose few long hub lists are latency-bound, the many-warp ones
+    // wide stages; 64-row batches (FP32 only: FP64 would need 256 registers
+    // for the two batches in flight) halve the work around the adds
     constexpr bool D = sizeof(T) == 8;
     switch (variant) {
     case 1: launch_hub_exact_v<T, 4, 6>(h, sm_count, st); break;
     case 2: launch_hub_exact_v<T, D ? 2 : 4, 12>(h, sm_count, st); break;
     case 3: launch_hub_exact_v<T, D ? 1 : 2, 24>(h, sm_count, st); break;
+    case 4:
+        if constexpr (D) launch_hub_exact_v<T, 2, 6>(h, sm_count, st);
+        else launch_hub_exact_v<T, 2, 12, 64>(h, sm_count, st);
+        break;
+    case 5:
+        if constexpr (D) launch_hub_exact_v<T, 1, 12>(h, sm_count, st);
+        else launch_hub_exact_v<T, 4, 6, 64>(h, sm_count, st);
+        break;
     default: launch_hub_exact_v<T, D ? 4 : 8, D ? 3 : 6>(h, sm_count, st); break;
     }
 }

@@ -705,36 +705,38 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
 
 // ---------------------------------------------------------------------------
 // Exact-order hub aggregation.  item = (hub vertex, group of 32 columns), one
-// warp per item.  The sum of a column over a hub's neighbour list in list
+// warp per item, neighbours in batches of BR (32 or 64).  The sum of a column over a hub's neighbour list in list
 // order -- the reference's order (CSCGraph.hpp:242-307), so the row equals
 // the per-tile aggregation bit for bit -- is one dependent chain of tens of
 // thousands of adds, fed by loads whose latency must be hidden:
-//   copies: the 32-column slices of a batch of 32 neighbours go straight into
+//   copies: the 32-column slices of a batch of BR neighbours go straight into
 //           a shared-memory tile (row u = neighbour u's slice) with cp.async,
 //           16 bytes a lane, a copy instruction moving whole slices (full
 //           sectors), NSLOT batches ahead (a ring of tiles per warp);
-//   adds:   lane l reads column l of the 32 rows (conflict-free shared loads)
+//   adds:   lane l reads column l of the BR rows (conflict-free shared loads)
 //           one batch ahead and adds them in order.
-// Neighbour ids travel through the same pipeline: lane l copies id l of a
-// batch (cp.async, 4 bytes) into a ring of NSLOT + 1 id slots, in the commit
+// Neighbour ids travel through the same pipeline: lane l copies ids l, l + 32,
+// ... of a batch (cp.async, 4 bytes) into a ring of NSLOT + 1 id slots, in the commit
 // group of the rows of the batch NSLOT earlier, so no step waits on a global
 // load: every wait is cp.async.wait_group for a group issued NSLOT - 2
 // batches earlier.  A lane waits for its own copies and __syncwarp makes the
 // whole tile (and id slot) visible; the rings belong to the warp, so nothing
 // wider is synchronised.  The result is the hub's single partial row (row v:
-// every hub is one chunk).
+// every hub is one chunk).  Batches of 64 halve the per-batch work around the
+// adds (one wait, commit and slot update for 64 neighbours) at twice the
+// registers and tile bytes.
 // ---------------------------------------------------------------------------
 // row stride (elements) of a staging tile: a multiple of 16 bytes whose word
 // offset between rows is 4 mod 32, so that the column reads are free of bank
 // conflicts (a copy phase of eight lanes writes 128 contiguous bytes)
 template <typename T> __host__ __device__ constexpr int hub_stage_stride() { return sizeof(T) == 4 ? 36 : 34; }
-template <typename T> __host__ __device__ constexpr int hub_tile_elems() { return 32 * hub_stage_stride<T>(); }
-// id slots of a warp's ring (one batch of 32 ids each)
+template <typename T, int BR = 32> __host__ __device__ constexpr int hub_tile_elems() { return BR * hub_stage_stride<T>(); }
+// id slots of a warp's ring (one batch of BR ids each)
 template <int NSLOT> __host__ __device__ constexpr int hub_id_slots() { return NSLOT + 1; }
 // shared-memory bytes of one warp: the tile ring and the id ring
-template <typename T, int NSLOT> __host__ __device__ constexpr size_t hub_warp_bytes()
+template <typename T, int NSLOT, int BR = 32> __host__ __device__ constexpr size_t hub_warp_bytes()
 {
-    return (size_t)NSLOT * hub_tile_elems<T>() * sizeof(T) + (size_t)hub_id_slots<NSLOT>() * 32 * sizeof(int32_t);
+    return (size_t)NSLOT * hub_tile_elems<T, BR>() * sizeof(T) + (size_t)hub_id_slots<NSLOT>() * BR * sizeof(int32_t);
 }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
@@ -769,18 +771,19 @@ __device__ __forceinline__ void cp_async4_zs(uint32_t sa, const void *gmem, uint
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-template <typename T, int NSLOT>
+template <typename T, int NSLOT, int BR>
 __device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, unsigned char *wsmem)
 {
     static_assert(NSLOT >= 3, "one batch in flight besides the two in registers");
+    static_assert(BR == 32 || BR == 64, "batches of 32 or 64 neighbours");
     constexpr int SS = hub_stage_stride<T>();
-    constexpr int TILE = hub_tile_elems<T>();
+    constexpr int TILE = hub_tile_elems<T, BR>();
     constexpr int PC = 16 / sizeof(T);   // columns per 16-byte piece
     constexpr int NP = 32 / PC;          // pieces per 32-column slice = lanes per neighbour of one copy
     constexpr int NPI = 32 / NP;         // neighbours per warp copy (whole 128-/256-byte slices)
-    constexpr int RPL = 32 / NPI;        // rows per lane group = copies per batch
+    constexpr int RPL = BR / NPI;        // rows per lane group = copies per batch
     constexpr int IDR = hub_id_slots<NSLOT>();
-    constexpr uint32_t TILE_B = TILE * sizeof(T), IDS_B = 32 * sizeof(int32_t);
+    constexpr uint32_t TILE_B = TILE * sizeof(T), IDS_B = BR * sizeof(int32_t);
     const T *ring = reinterpret_cast<const T *>(wsmem);
     const int32_t *ids = reinterpret_cast<const int32_t *>(wsmem + (size_t)NSLOT * TILE_B);
     const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(wsmem);
@@ -794,7 +797,7 @@ __device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, unsig
     const int c0 = grp * 32;                                   // first column of the slice
     const bool lr_in = c0 + (lr + 1) * PC <= h.aux_pitch;      // this lane's piece lies inside the row
     const int beg = __ldg(h.off + v), deg = __ldg(h.off + v + 1) - beg;
-    const int nbt = (deg + 31) / 32;
+    const int nbt = (deg + BR - 1) / BR;
     // this lane's piece of row 0 (a lane whose piece lies past the row copies
     // the slice's first piece instead: columns past the row are never
     // written out), and its first tile row in slot 0
@@ -802,12 +805,15 @@ __device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, unsig
     const uint32_t row_bytes = (uint32_t)h.aux_pitch * (uint32_t)sizeof(T);
     const uint32_t dst0 = ring_s + (uint32_t)((ln * RPL * SS + lr * PC) * sizeof(T));
     const int32_t *adj_v = h.adj + beg;
-    // id `lane` of batch j into the id slot at byte offset `slot_b` (zero past
-    // the list: a valid row that is never added)
+    // ids lane, lane + 32, ... of batch j into the id slot at byte offset
+    // `slot_b` (zero past the list: a valid row that is never added)
     auto fetch_ids = [&](int j, uint32_t slot_b) {
-        const int e = j * 32 + lane;
-        const bool in = e < deg;
-        cp_async4_zs(ids_s + slot_b + lane * 4, adj_v + (in ? e : 0), in ? 4u : 0u);
+#pragma unroll
+        for (int i = 0; i < BR / 32; ++i) {
+            const int e = j * BR + i * 32 + lane;
+            const bool in = e < deg;
+            cp_async4_zs(ids_s + slot_b + (i * 32 + lane) * 4, adj_v + (in ? e : 0), in ? 4u : 0u);
+        }
     };
     // A batch's copy plan for this lane: the source of each of its RPL pieces.
     uint64_t src[RPL];
@@ -825,9 +831,9 @@ __device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, unsig
     // batch b's copies into the ring slot at byte offset ts_b: every row of a
     // full batch, the rows inside the list of the last one, none past it
     auto copy = [&](int b, uint32_t ts_b) {
-        const int left = deg - b * 32;
+        const int left = deg - b * BR;
         const uint32_t d = dst0 + ts_b;
-        if (left >= 32) {
+        if (left >= BR) {
 #pragma unroll
             for (int k = 0; k < RPL; ++k) cp_async16_s(d + (uint32_t)(k * SS * sizeof(T)), reinterpret_cast<const void *>(src[k]));
         } else if (left > 0) {
@@ -837,10 +843,10 @@ __device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, unsig
                     cp_async16_s(d + (uint32_t)(k * SS * sizeof(T)), reinterpret_cast<const void *>(src[k]));
         }
     };
-    auto load = [&](T(&x)[32], uint32_t ts_b) {
+    auto load = [&](T(&x)[BR], uint32_t ts_b) {
         const T *tile = ring + ts_b / sizeof(T) + lane;
 #pragma unroll
-        for (int u = 0; u < 32; ++u) x[u] = tile[u * SS];
+        for (int u = 0; u < BR; ++u) x[u] = tile[u * SS];
     };
     // ids of batches 0 .. NSLOT - 1 first; batch j >= NSLOT has its ids
     // fetched with batch j - NSLOT's rows, into the slot of batch j - NSLOT - 1
@@ -866,7 +872,7 @@ __device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, unsig
     // the last batch under a predicate.  Slots (byte offsets) advance by one.
     uint32_t ts_b = (NSLOT - 1) * TILE_B, is_b = (NSLOT - 1) * IDS_B, ls_b = TILE_B;
     T acc = T(0);
-    auto step = [&](int b, T(&cur)[32], T(&nxt)[32], bool tail, bool last) {
+    auto step = [&](int b, T(&cur)[BR], T(&nxt)[BR], bool tail, bool last) {
         if (!tail) {
 #pragma unroll
             for (int k = 0; k < RPL; ++k)
@@ -885,15 +891,15 @@ __device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, unsig
         plan(is_b);                   // batch b + NSLOT: its ids landed with batch b's rows
         if (!last) {
 #pragma unroll
-            for (int u = 0; u < 32; ++u) acc = add_rn(acc, cur[u]);
+            for (int u = 0; u < BR; ++u) acc = add_rn(acc, cur[u]);
         } else {
-            const int n = deg - b * 32;
+            const int n = deg - b * BR;
 #pragma unroll
-            for (int u = 0; u < 32; ++u)
+            for (int u = 0; u < BR; ++u)
                 if (u < n) acc = add_rn(acc, cur[u]);
         }
     };
-    T x[32], y[32];
+    T x[BR], y[BR];
     cp_async_wait<NSLOT - 2>();   // batch 0
     __syncwarp();
     load(x, 0);
