@@ -113,6 +113,13 @@ sg_status sg_plan_tables(sg_plan p, int32_t s, int32_t *c2c, int32_t *msplit, in
 sg_status sg_plan_automorphisms(sg_plan p, int32_t *count);
 /* the edges of sub s's relabelled subtree (DivideTemplates::get_subtps) */
 sg_status sg_plan_sub_edges(sg_plan p, int32_t s, int32_t *n, int32_t *src, int32_t *dst);
+/* Tables computed once (no counterpart in the reference, which computes every
+ * sub): same_as[s] (nsub entries) = the sub processed before s whose table
+ * equals s's -- the same rooted split structure below it and the same
+ * position relative to the 1e-12-scaled sub -- so s reuses that table and is
+ * not computed again; -1 when s computes its own (every sub in the isPruned=0
+ * CSC mode, whose running buffer makes each step's table its own). */
+sg_status sg_plan_shared_tables(sg_plan p, int32_t *same_as);
 
 /* ---- device graph -------------------------------------------------------- */
 

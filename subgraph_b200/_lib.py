@@ -30,7 +30,7 @@ EXPORTS = [
     "sg_edgelist_read", "sg_edgelist_write", "sg_csc_build", "sg_csr_build",
     "sg_graph_data_write", "sg_graph_data_read", "sg_graph_data_encode", "sg_graph_data_decode",
     "sg_rmat_generate",
-    "sg_plan_create", "sg_plan_read", "sg_plan_destroy", "sg_plan_info", "sg_plan_sub",
+    "sg_plan_create", "sg_plan_read", "sg_plan_destroy", "sg_plan_info", "sg_plan_sub", "sg_plan_shared_tables",
     "sg_plan_tables", "sg_plan_automorphisms", "sg_plan_sub_edges",
     "sg_graph_create", "sg_graph_destroy", "sg_graph_info", "sg_graph_create_edges", "sg_graph_create_text",
     "sg_graph_create_rmat", "sg_graph_download_csc",
@@ -96,6 +96,7 @@ def lib() -> ctypes.CDLL:
         "sg_plan_destroy": ([vp], None),
         "sg_plan_info": ([vp, P(i32), P(i32), P(i32), P(i64)], i32),
         "sg_plan_sub": ([vp, i32, vp], i32),
+        "sg_plan_shared_tables": ([vp, vp], i32),
         "sg_plan_tables": ([vp, i32, vp, vp, vp], i32),
         "sg_plan_automorphisms": ([vp, P(i32)], i32),
         "sg_plan_sub_edges": ([vp, i32, P(i32), vp, vp], i32),

@@ -353,6 +353,14 @@ class Graph:
         check(lib().sg_plan_automorphisms(self.plan, ctypes.byref(c)))
         return c.value
 
+    def shared_tables(self) -> list[int]:
+        """Per sub: the sub processed before it whose table it reuses, or -1."""
+        k, ns = ctypes.c_int32(), ctypes.c_int32()
+        check(lib().sg_plan_info(self.plan, ctypes.byref(k), ctypes.byref(ns), None, None))
+        out = np.zeros(ns.value, np.int32)
+        check(lib().sg_plan_shared_tables(self.plan, _p(out)))
+        return [int(x) for x in out]
+
 
 class DivideTemplates:
     """Sub-template chain of a template (DivideTemplates.hpp:13-64)."""

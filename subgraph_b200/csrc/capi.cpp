@@ -303,6 +303,13 @@ sg_status sg_plan_automorphisms(sg_plan p, int32_t *count)
     return SG_OK;
 }
 
+sg_status sg_plan_shared_tables(sg_plan p, int32_t *same_as)
+{
+    if (!p || !same_as) return fail(SG_ERR_INVALID, "null argument");
+    for (int s = 0; s < p->p.nsub(); ++s) same_as[s] = p->p.same_as[s];
+    return SG_OK;
+}
+
 sg_status sg_plan_sub_edges(sg_plan p, int32_t s, int32_t *n, int32_t *src, int32_t *dst)
 {
     if (!p || !n) return fail(SG_ERR_INVALID, "null argument");

@@ -798,7 +798,7 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
     GraphState &gs = c.gs;
     Workspace &w = gs.ws;
     const size_t V = (size_t)g.V;
-    c.arena_per_coloring = (size_t)c.p.arena_units * V * c.es;
+    c.arena_per_coloring = (size_t)(c.mode == kModeOriginal ? c.p.arena_units_all : c.p.arena_units) * V * c.es;
     SG_CKS(grow(&w.arena, &w.arena_bytes, std::max<size_t>(16, c.arena_per_coloring * ncolor_slots), g.stream));
     SG_CKS(growT(&w.colors, &w.colors_bytes, std::max<size_t>(16, V * ncolor_slots), g.stream));
     SG_CKS(growT(&w.partial, &w.partial_bytes, 8 * ((V / 8 + 2) * ncolor_slots), g.stream));
@@ -828,9 +828,13 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
 // the table is [V][lay][pitch] at lay times the per-coloring offset.
 void *table_ptr(RunCtx &c, int slot, int sub)
 {
-    return (char *)c.gs.ws.arena + c.arena_base + c.arena_per_coloring * slot +
-           (size_t)c.lay * c.p.table_offset[sub] * c.g.V * c.es;
+    const int64_t off = c.mode == kModeOriginal ? c.p.table_offset_all[sub] : c.p.table_offset[sub];
+    return (char *)c.gs.ws.arena + c.arena_base + c.arena_per_coloring * slot + (size_t)c.lay * off * c.g.V * c.es;
 }
+
+// A sub whose table an earlier sub of the same structure already computed
+// (Plan::same_as) is not run again; the isPruned=0 CSC mode runs every sub.
+bool shared_table(const RunCtx &c, int s) { return c.mode != kModeOriginal && c.p.same_as[s] >= 0; }
 
 // neighbour ids with their color in the top 4 bits: ids below 2^28, colors below 16
 bool adjc_ok(const DeviceGraph &g, const Plan &p) { return g.V < (1 << 28) && p.k <= 16 && g.nnz > 0; }
@@ -984,6 +988,7 @@ Status run_stage_original(RunCtx &c, int slot, int s, double *root_vertex, cudaS
 Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t st, int b0 = 0, int nb = 1)
 {
     if (c.mode == kModeOriginal) return run_stage_original(c, slot, s, root_vertex, st);
+    if (shared_table(c, s)) return Status::ok();
     DeviceGraph &g = c.g;
     StageDesc d = make_stage(c, slot, s, root_vertex, b0, nb);
     if (c.hubs.count > 0) {
@@ -1274,6 +1279,10 @@ Status add_queue_stage(RunCtx &c, int slot, int s, void *hub_region, QueueSlot &
 {
     const Plan &p = c.p;
     const SubTemplate &sub = p.subs[s];
+    if (shared_table(c, s)) {   // its readers wait for the sub that computes the table
+        q.fused[s] = q.fused[p.same_as[s]];
+        return Status::ok();
+    }
     StageDesc d = make_stage(c, slot, s, nullptr);
     if (c.hubs.count > 0) {
         BatchStage hs{};
@@ -1495,6 +1504,7 @@ std::map<std::string, int> g_group_nb;
 
 Status run_stage_group(RunCtx &c, int s, cudaStream_t st)
 {
+    if (shared_table(c, s)) return Status::ok();
     const int L = c.lay;
     auto pass = [&](int nb) -> Status {
         for (int b0 = 0; b0 < L; b0 += nb) SG_CKS(run_stage(c, 0, s, nullptr, st, b0, std::min(nb, L - b0)));

@@ -19,6 +19,7 @@
 #include <deque>
 #include <functional>
 #include <map>
+#include <string>
 
 namespace sg {
 
@@ -275,53 +276,103 @@ bool make_plan(const Template &t, Plan &p, std::string &err)
             p.process_order.push_back(si);
             if (p.scaled_sub < 0) p.scaled_sub = si;
         }
-    // ---- count-table arena: tables live from their sub's step to their parent's
-    p.table_offset.assign(ns, -1);
-    p.table_pitch.assign(ns, 0);
-    std::vector<std::pair<int64_t, int64_t>> freel;   // (offset, length), sorted
-    int64_t top = 0;
-    auto alloc = [&](int64_t len) {
-        for (size_t i = 0; i < freel.size(); ++i)
-            if (freel[i].second >= len) {
-                int64_t off = freel[i].first;
-                freel[i].first += len;
-                freel[i].second -= len;
-                if (freel[i].second == 0) freel.erase(freel.begin() + i);
-                return off;
-            }
-        int64_t off = top;
-        top += len;
-        return off;
-    };
-    auto release = [&](int64_t off, int64_t len) {
-        freel.push_back({off, len});
-        std::sort(freel.begin(), freel.end());
-        std::vector<std::pair<int64_t, int64_t>> merged;
-        for (auto &f : freel) {
-            if (!merged.empty() && merged.back().first + merged.back().second == f.first) merged.back().second += f.second;
-            else merged.push_back(f);
+    // ---- tables computed once.  A sub's table is a function of its rooted
+    // shape and split structure (its main and aux children's, recursively: the
+    // splits, the index tables and every operand follow from them) and of
+    // whether the scaled sub lies below it (its 1e-12 reaches every table
+    // above it), so two subs with the same signature have equal tables.
+    // Children have higher indices and are processed first.
+    {
+        std::vector<std::string> sig(ns);
+        for (int si = ns - 1; si >= 0; --si) {
+            const SubTemplate &s = p.subs[si];
+            sig[si] = s.size == 1 ? std::string("1")
+                                  : "(" + sig[s.main] + "," + sig[s.aux] + ")" + (si == p.scaled_sub ? "s" : "");
         }
-        if (!merged.empty() && merged.back().first + merged.back().second == top) { top = merged.back().first; merged.pop_back(); }
-        freel.swap(merged);
-    };
-    int64_t peak = 0;
-    for (int si : p.process_order) {
-        SubTemplate &s = p.subs[si];
-        if (si > 0) {
-            // rows an aggregation gathers (the parent's aux child) are 32-byte
-            // aligned for its 256-bit loads; main-child rows, read element by
-            // element, keep 16-byte rows
-            const bool gathered = s.parent >= 0 && s.parent < ns && p.subs[s.parent].aux == si;
-            p.table_pitch[si] = gathered ? (s.L + 7) / 8 * 8 : (s.L + 3) / 4 * 4;
-            // arena slots are whole multiples of 8 units, so every table starts
-            // 32-byte aligned for any V
-            p.table_offset[si] = alloc((p.table_pitch[si] + 7) / 8 * 8);
-            peak = std::max(peak, top);
+        p.same_as.assign(ns, -1);
+        std::map<std::string, int> first;
+        for (int si : p.process_order) {
+            if (si == 0) continue;   // the root has no table
+            auto it = first.find(sig[si]);
+            if (it == first.end()) first.emplace(sig[si], si);
+            else p.same_as[si] = it->second;
         }
-        for (int c : {s.main, s.aux})
-            if (p.subs[c].size > 1) release(p.table_offset[c], (p.table_pitch[c] + 7) / 8 * 8);
     }
-    p.arena_units = peak;
+    // ---- count-table arena: a table lives from its sub's step to its last
+    // reader's (its parent's; for a shared table, the last of its subs'
+    // parents).  Rows an aggregation gathers (a parent's aux child) are
+    // 32-byte aligned for its 256-bit loads; main-child rows, read element by
+    // element, keep 16-byte rows; a shared table takes the wider of its subs'.
+    p.table_pitch.assign(ns, 0);
+    {
+        std::vector<int> need8(ns, 0);
+        for (int si : p.process_order) {
+            if (si == 0) continue;
+            const SubTemplate &s = p.subs[si];
+            const int r = p.same_as[si] >= 0 ? p.same_as[si] : si;
+            if (s.parent >= 0 && s.parent < ns && p.subs[s.parent].aux == si) need8[r] = 1;
+        }
+        for (int si : p.process_order) {
+            if (si == 0) continue;
+            const int r = p.same_as[si] >= 0 ? p.same_as[si] : si;
+            const int L = p.subs[si].L;
+            p.table_pitch[si] = need8[r] ? (L + 7) / 8 * 8 : (L + 3) / 4 * 4;
+        }
+    }
+    auto plan_arena = [&](bool share, std::vector<int64_t> &offset, int64_t &units) {
+        offset.assign(ns, -1);
+        std::vector<std::pair<int64_t, int64_t>> freel;   // (offset, length), sorted
+        int64_t top = 0;
+        auto alloc = [&](int64_t len) {
+            for (size_t i = 0; i < freel.size(); ++i)
+                if (freel[i].second >= len) {
+                    int64_t off = freel[i].first;
+                    freel[i].first += len;
+                    freel[i].second -= len;
+                    if (freel[i].second == 0) freel.erase(freel.begin() + i);
+                    return off;
+                }
+            int64_t off = top;
+            top += len;
+            return off;
+        };
+        auto release = [&](int64_t off, int64_t len) {
+            freel.push_back({off, len});
+            std::sort(freel.begin(), freel.end());
+            std::vector<std::pair<int64_t, int64_t>> merged;
+            for (auto &f : freel) {
+                if (!merged.empty() && merged.back().first + merged.back().second == f.first)
+                    merged.back().second += f.second;
+                else merged.push_back(f);
+            }
+            if (!merged.empty() && merged.back().first + merged.back().second == top) {
+                top = merged.back().first;
+                merged.pop_back();
+            }
+            freel.swap(merged);
+        };
+        auto owner = [&](int si) { return share && p.same_as[si] >= 0 ? p.same_as[si] : si; };
+        std::vector<int> readers(ns, 0);   // per owning sub: parents still to run
+        for (int si : p.process_order)
+            if (si != 0) ++readers[owner(si)];
+        int64_t peak = 0;
+        for (int si : p.process_order) {
+            const SubTemplate &s = p.subs[si];
+            if (si > 0) {
+                // arena slots are whole multiples of 8 units, so every table
+                // starts 32-byte aligned for any V
+                if (owner(si) != si) offset[si] = offset[owner(si)];
+                else offset[si] = alloc((p.table_pitch[si] + 7) / 8 * 8);
+                peak = std::max(peak, top);
+            }
+            for (int c : {s.main, s.aux})
+                if (p.subs[c].size > 1 && --readers[owner(c)] == 0)
+                    release(offset[owner(c)], (p.table_pitch[c] + 7) / 8 * 8);
+        }
+        units = peak;
+    };
+    plan_arena(true, p.table_offset, p.arena_units);
+    plan_arena(false, p.table_offset_all, p.arena_units_all);
     p.automorphisms = 1;
     static std::atomic<uint64_t> next_uid{1};
     p.uid = next_uid++;

@@ -42,10 +42,19 @@ struct Plan {
     int scaled_sub = -1;                 // the first non-bottom sub processed (1e-12 scale)
     int automorphisms = 1;
 
+    // Tables computed once: same_as[s] = a sub processed before s whose table
+    // equals s's (the same rooted split structure all the way down and the same
+    // position relative to the scaled sub), else -1.  Such subs share one table.
+    std::vector<int> same_as;
+
     // count-table arena, in units of "V elements" (a table of pitch P uses P units)
-    std::vector<int64_t> table_offset;   // per sub, -1 when the sub has no table
+    std::vector<int64_t> table_offset;   // per sub (shared tables at one offset), -1 when the sub has no table
     std::vector<int32_t> table_pitch;    // row pitch (elements): multiple of 8 for aux children, else of 4
     int64_t arena_units = 0;
+    // the arena with every sub's table computed and held on its own (the
+    // isPruned=0 CSC mode, whose running buffer makes each step's table differ)
+    std::vector<int64_t> table_offset_all;
+    int64_t arena_units_all = 0;
 
     int nsub() const { return (int)subs.size(); }
 };

@@ -237,3 +237,45 @@ def test_csr_build_matches_reference():
         g.createFromEdgeListFile(V, len(src), src, dst)
         assert np.array_equal(g.getIndexRow(), row), name
         assert np.array_equal(g.getIndexCol(), col), name
+
+
+def _signature(P, s, scaled):
+    """A sub's table signature: its rooted split structure and whether the
+    1e-12-scaled sub lies below it (the oracle's own DivideTemplates)."""
+    if P.subs[s].size == 1:
+        return "1"
+    return "(" + _signature(P, P.subs[s].main, scaled) + "," + _signature(P, P.subs[s].aux, scaled) + ")" + (
+        "s" if s == scaled else "")
+
+
+def test_shared_tables_are_subs_of_equal_signature():
+    """A sub reuses the table of an earlier-processed sub exactly when both have
+    the same split structure below them and the same relation to the scaled
+    sub (the 12-vertex tree: its three unscaled 2-colour subs share one table;
+    a 9-vertex tree whose size-3 subs differ only by the scaled sub beneath one
+    of them shares nothing)."""
+    t12 = sg.Graph(*TEMPLATES["tree12"])
+    same = t12.shared_tables()
+    assert [s for s, x in enumerate(same) if x >= 0] == [5, 11] and same[5] == same[11] == 16
+    t9 = sg.Graph(9, [(2, 3), (4, 1), (7, 1), (1, 0), (0, 6), (6, 5), (5, 3), (3, 8)])
+    assert all(x < 0 for x in t9.shared_tables())
+    rng = random.Random(77)
+    for _ in range(60):
+        n = rng.randint(3, 14)
+        edges = prufer_tree(n, rng)
+        t = sg.Graph(n, edges)
+        same = t.shared_tables()
+        P = O.Plan(n, edges)
+        order = [s for s in range(len(P.subs) - 1, -1, -1) if P.subs[s].size > 1]
+        scaled = order[0]   # the first non-bottom sub processed (CountMat.cpp:813-822)
+        seen = {}
+        for s in order:
+            if s == 0:
+                assert same[s] == -1
+                continue
+            sig = _signature(P, s, scaled)
+            if sig in seen:
+                assert same[s] == seen[sig], (n, edges, s)
+            else:
+                assert same[s] == -1, (n, edges, s)
+                seen[sig] = s
