@@ -261,13 +261,15 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
         // per-color neighbour counts (row b*k + c for coloring b): one thread per
         // (vertex, coloring), each owning its k counters (exact integers, no
         // atomics), neighbours in predicated batches of 8 with their loads in
-        // flight together
+        // flight together.  The colorings of a vertex are adjacent threads, so
+        // that they share the neighbour ids and read the neighbour's colours
+        // ([V][nb] bytes) together.
         const int nk = nbc * d.k;
         for (int vi = tid; vi < tv; vi += NT)
             for (int c = 0; c < nk; ++c) agg_s[c * RS + vi] = T(0);
         __syncthreads();
         for (int idx = tid; idx < nbc * tv; idx += NT) {
-            const int b = idx / tv, vi = idx - b * tv;
+            const int vi = idx / nbc, b = idx - vi * nbc;
             const int v = v0 + vi;
             T *cnt = agg_s + (size_t)b * d.k * RS + vi;
             if (v < d.hub_count) {
