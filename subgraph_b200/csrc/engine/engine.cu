@@ -105,6 +105,8 @@ struct Workspace {
     size_t adjc_bytes = 0;
     float *orig_buf = nullptr;         // [V] isPruned=0 (CSC) aggregation buffer, internal order
     size_t orig_buf_bytes = 0;
+    int32_t *hub_ticket = nullptr;     // exact-order hub kernel's item counters, one per concurrent stream
+    size_t hub_ticket_bytes = 0;
     uint64_t generation = 0;   // bumped whenever a buffer above is re-allocated
 };
 
@@ -574,7 +576,8 @@ DeviceGraph::~DeviceGraph()
         if (it != g_state.end()) {
             Workspace &w = it->second.ws;
             for (void *p : {w.arena, (void *)w.colors, (void *)w.partial, (void *)w.raw, (void *)w.windows, w.hub_partial,
-                            (void *)w.chunk_start, (void *)w.root_vertex, (void *)w.adjc, (void *)w.orig_buf})
+                            (void *)w.chunk_start, (void *)w.root_vertex, (void *)w.adjc, (void *)w.orig_buf,
+                            (void *)w.hub_ticket})
                 if (p) cudaFreeAsync(p, stream);
             for (auto &kv : it->second.plans) {
                 for (auto *p : kv.second.split) if (p) cudaFreeAsync(p, stream);
@@ -739,6 +742,7 @@ struct RunCtx {
     bool exact = false;      // no fused products (packed eMA), no hub chunks
     bool use_adjc = false;   // one coloring at a time per slot: neighbour ids carry their colors
     void *hub_region = nullptr;  // this context's hub partial rows (job streams), else the workspace's
+    int ticket = 0;              // its exact-order hub item counter (job streams: the stream's)
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> fused_ev, hub_ev;
     std::vector<std::pair<int, double>> fused_sub;   // per fused launch: sub, compulsory bytes
     double fused_alg_bytes = 0, fused_gather_bytes = 0;
@@ -820,6 +824,7 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
         for (int h = 0; h < c.hubs.count; ++h) cs[h + 1] = cs[h] + (g.h_degree[h] + c.hubs.chunk - 1) / c.hubs.chunk;
         SG_CKS(growT(&w.chunk_start, &w.chunk_start_bytes, 4 * cs.size(), g.stream));
         SG_CK(cudaMemcpyAsync(w.chunk_start, cs.data(), 4 * cs.size(), cudaMemcpyHostToDevice, g.stream));
+        SG_CKS(growT(&w.hub_ticket, &w.hub_ticket_bytes, 4 * 64, g.stream));
     }
     return Status::ok();
 }
@@ -941,6 +946,7 @@ HubArgs make_hub(RunCtx &c, StageDesc &d, void *partial)
     h.adj = g.d_adj;
     h.aux = d.aux;
     h.partial = partial;
+    h.ticket = c.gs.ws.hub_ticket ? c.gs.ws.hub_ticket + c.ticket : nullptr;
     d.hub_count = c.hubs.count;
     d.hub_pitch = c.hub_pitch;
     d.hub_chunk_start = c.gs.ws.chunk_start;
@@ -2050,6 +2056,7 @@ Status count_jobs_streams(DeviceGraph &g, const std::vector<const Plan *> &plans
         for (int h = 0; h < hubs.count; ++h) cs[h + 1] = cs[h] + (g.h_degree[h] + hubs.chunk - 1) / hubs.chunk;
         SG_CKS(growT(&w.chunk_start, &w.chunk_start_bytes, 4 * cs.size(), st));
         SG_CK(cudaMemcpyAsync(w.chunk_start, cs.data(), 4 * cs.size(), cudaMemcpyHostToDevice, st));
+        SG_CKS(growT(&w.hub_ticket, &w.hub_ticket_bytes, 4 * (size_t)std::max(64, S), st));
         SG_CK(cudaStreamSynchronize(st));   // `cs` is pageable and goes out of scope
     }
     {
@@ -2081,6 +2088,7 @@ Status count_jobs_streams(DeviceGraph &g, const std::vector<const Plan *> &plans
         cudaStream_t js = gs.streams[s];
         RunCtx &c = ctx[j];
         c.hub_region = hubs.count > 0 ? (char *)w.hub_partial + hub_region * s : nullptr;
+        c.ticket = s;
         status = launch_colors(c, s, j, 1, js);
         for (int sub : c.p.process_order)
             if (!status.code) status = run_stage(c, s, sub, nullptr, js);

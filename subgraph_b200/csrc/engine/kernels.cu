@@ -119,15 +119,23 @@ __global__ void __launch_bounds__(NT) k_hub(HubArgs h)
 // autotuner picks one per row width.
 int hub_variants() { return 6; }
 
+// Items are taken from a ticket counter: every warp takes the next item when
+// it is done with its last, so the long lists (the first items) do not end up
+// behind a fixed share of the others on the same warp.
 template <typename T, int W, int NSLOT, int BR>
 __global__ void __launch_bounds__(32 * W) k_hub_exact(HubArgs h)
 {
     extern __shared__ __align__(32) unsigned char smem_raw[];
-    const int warp = threadIdx.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char *wsmem = smem_raw + (size_t)warp * hub_warp_bytes<T, NSLOT, BR>();
     const int items = h.hub_count * ((h.L_a + 31) / 32);
-    for (int item = blockIdx.x * W + warp; item < items; item += gridDim.x * W)
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(h.ticket, 1);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= items) break;
         hub_item_exact<T, NSLOT, BR>(h, item, wsmem);
+    }
 }
 
 template <typename T, int W, int NSLOT, int BR = 32>
@@ -142,6 +150,7 @@ static void launch_hub_exact_v(const HubArgs &h, int sm_count, cudaStream_t st)
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * W, smem) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     const int grid = std::max(1, std::min((items + W - 1) / W, sm_count * per_sm));
+    cudaMemsetAsync(h.ticket, 0, sizeof(int32_t), st);
     kern<<<grid, 32 * W, smem, st>>>(h);
 }
 

@@ -119,6 +119,7 @@ struct HubArgs {
     // are split among lanes, each lane summing its columns over the whole
     // neighbour list in order -- the reference's summation order
     int32_t exact_order;
+    int32_t *ticket;             // exact order: the next item to take (zeroed before each launch)
 };
 
 // ---------------------------------------------------------------------------
