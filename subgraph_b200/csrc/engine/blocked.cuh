@@ -22,6 +22,17 @@ __global__ void __launch_bounds__(NT, (NT == 512 ? blk_min_blocks<N, P>() : 2 * 
     k_fused_blk(StageDesc d)
 {
     extern __shared__ __align__(32) unsigned char smem_raw[];
+    if (d.ticket) {   // dynamic tiles, as k_fused
+        __shared__ int s_tile;
+        for (;;) {
+            if (threadIdx.x == 0) s_tile = d.tile_begin + atomicAdd(d.ticket, 1);
+            __syncthreads();
+            const int tile = s_tile;
+            if (tile >= d.ntiles) break;
+            fused_tile<float, NT, Q, false, false, true, N, P>(d, tile, smem_raw);
+        }
+        return;
+    }
     for (int tile = d.tile_begin + blockIdx.x; tile < d.ntiles; tile += gridDim.x)
         fused_tile<float, NT, Q, false, false, true, N, P>(d, tile, smem_raw);
 }
@@ -35,6 +46,7 @@ static void launch_blk_q(const StageDesc &d, const FusedConfig &cfg, cudaStream_
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, cfg.smem) != cudaSuccess || per_sm < 1)
             per_sm = 1;
         const int grid = std::max(1, std::min(d.ntiles - d.tile_begin, cfg.grid * per_sm));
+        if (d.ticket) cudaMemsetAsync(d.ticket, 0, sizeof(int32_t), st);
         kern<<<grid, NT, cfg.smem, st>>>(d);
     };
     switch (d.gather_q) {

@@ -107,6 +107,8 @@ struct Workspace {
     size_t orig_buf_bytes = 0;
     int32_t *hub_ticket = nullptr;     // exact-order hub kernel's item counters, one per concurrent stream
     size_t hub_ticket_bytes = 0;
+    int32_t *tile_ticket = nullptr;    // fused kernels' tile counters, one per concurrent stream
+    size_t tile_ticket_bytes = 0;
     uint64_t generation = 0;   // bumped whenever a buffer above is re-allocated
 };
 
@@ -577,7 +579,7 @@ DeviceGraph::~DeviceGraph()
             Workspace &w = it->second.ws;
             for (void *p : {w.arena, (void *)w.colors, (void *)w.partial, (void *)w.raw, (void *)w.windows, w.hub_partial,
                             (void *)w.chunk_start, (void *)w.root_vertex, (void *)w.adjc, (void *)w.orig_buf,
-                            (void *)w.hub_ticket})
+                            (void *)w.hub_ticket, (void *)w.tile_ticket})
                 if (p) cudaFreeAsync(p, stream);
             for (auto &kv : it->second.plans) {
                 for (auto *p : kv.second.split) if (p) cudaFreeAsync(p, stream);
@@ -742,7 +744,7 @@ struct RunCtx {
     bool exact = false;      // no fused products (packed eMA), no hub chunks
     bool use_adjc = false;   // one coloring at a time per slot: neighbour ids carry their colors
     void *hub_region = nullptr;  // this context's hub partial rows (job streams), else the workspace's
-    int ticket = 0;              // its exact-order hub item counter (job streams: the stream's)
+    int ticket = 0;              // its hub item and tile counters (job streams: the stream's)
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> fused_ev, hub_ev;
     std::vector<std::pair<int, double>> fused_sub;   // per fused launch: sub, compulsory bytes
     double fused_alg_bytes = 0, fused_gather_bytes = 0;
@@ -805,6 +807,7 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
     c.arena_per_coloring = (size_t)(c.mode == kModeOriginal ? c.p.arena_units_all : c.p.arena_units) * V * c.es;
     SG_CKS(grow(&w.arena, &w.arena_bytes, std::max<size_t>(16, c.arena_per_coloring * ncolor_slots), g.stream));
     SG_CKS(growT(&w.colors, &w.colors_bytes, std::max<size_t>(16, V * ncolor_slots), g.stream));
+    SG_CKS(growT(&w.tile_ticket, &w.tile_ticket_bytes, 4 * 64, g.stream));
     SG_CKS(growT(&w.partial, &w.partial_bytes, 8 * ((V / 8 + 2) * ncolor_slots), g.stream));
     SG_CKS(growT(&w.raw, &w.raw_bytes, 8 * (size_t)std::max(ncolorings_total, 1), g.stream));
     SG_CKS(growT(&w.windows, &w.windows_bytes, 4 * 31 * (size_t)std::max(ncolorings_total, 1), g.stream));
@@ -859,6 +862,7 @@ StageDesc make_stage(RunCtx &c, int slot, int s, double *root_vertex, int b0 = 0
     d.L_s = sub.L;
     d.S = sub.S;
     d.k = p.k;
+    d.ticket = w.tile_ticket ? w.tile_ticket + c.ticket : nullptr;
     d.main_leaf = m.size == 1;
     d.aux_leaf = a.size == 1;
     d.L_m = m.L;
@@ -2059,6 +2063,7 @@ Status count_jobs_streams(DeviceGraph &g, const std::vector<const Plan *> &plans
         SG_CKS(growT(&w.hub_ticket, &w.hub_ticket_bytes, 4 * (size_t)std::max(64, S), st));
         SG_CK(cudaStreamSynchronize(st));   // `cs` is pageable and goes out of scope
     }
+    SG_CKS(growT(&w.tile_ticket, &w.tile_ticket_bytes, 4 * (size_t)std::max(64, S), st));
     {
         std::vector<uint32_t> win((size_t)n * 31);
         for (int j = 0; j < n; ++j) glibc_window(seeds[j], &win[(size_t)j * 31]);

@@ -102,6 +102,20 @@ template <typename T, int NT, int Q, bool PK>
 __global__ void __launch_bounds__(NT) k_fused(StageDesc d)
 {
     extern __shared__ __align__(32) unsigned char smem_raw[];
+    if (d.ticket) {
+        // tiles in vertex order (degree-descending: the heaviest first), each
+        // CTA taking the next one when it is done (fused_tile ends with a
+        // barrier, so the shared word is read before it is written again)
+        __shared__ int s_tile;
+        for (;;) {
+            if (threadIdx.x == 0) s_tile = d.tile_begin + atomicAdd(d.ticket, 1);
+            __syncthreads();
+            const int tile = s_tile;
+            if (tile >= d.ntiles) break;
+            fused_tile<T, NT, Q, PK>(d, tile, smem_raw);
+        }
+        return;
+    }
     for (int tile = d.tile_begin + blockIdx.x; tile < d.ntiles; tile += gridDim.x) fused_tile<T, NT, Q, PK>(d, tile, smem_raw);
 }
 
@@ -371,6 +385,7 @@ static void launch_fused_q(const StageDesc &d, const FusedConfig &cfg, cudaStrea
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, cfg.smem) != cudaSuccess || per_sm < 1)
             per_sm = 1;
         const int grid = std::max(1, std::min(d.ntiles - d.tile_begin, cfg.grid * per_sm));
+        if (d.ticket) cudaMemsetAsync(d.ticket, 0, sizeof(int32_t), st);
         kern<<<grid, NT, cfg.smem, st>>>(d);
     };
     if (d.packed == 1) {

@@ -42,6 +42,8 @@ struct StageDesc {
     int32_t gather_q;                  // 32-byte column chunks per thread (1, 2 or 4)
     int32_t ntiles;
     int32_t tile_begin;                // a launch covers tiles [tile_begin, ntiles)
+    int32_t *ticket;                   // non-null: CTAs take tiles from this counter (zeroed before the
+                                       // launch), else tile_begin + blockIdx.x, stride gridDim.x
     int32_t out_chunk;                 // outputs staged in shared memory per pass
     size_t smem;                       // dynamic shared memory bytes
     // vertices [0, hub_count) are aggregated by the hub kernel in neighbour
