@@ -943,6 +943,7 @@ HubArgs make_hub(RunCtx &c, StageDesc &d, void *partial)
     h.nb = d.nb;
     h.cstride = d.cstride;
     h.color = d.color;
+    h.adjc = d.adjc;
     h.total_chunks = c.hubs.total_chunks;
     h.chunk_start = c.gs.ws.chunk_start;
     h.exact_order = c.hubs.exact_order ? 1 : 0;

@@ -112,6 +112,7 @@ struct HubArgs {
     int32_t nb, cstride;         // k_leaf: colorings, color layout (color[v * cstride + b])
     int32_t total_chunks;
     const uint8_t *color;        // [V] internal order (k_leaf only)
+    const int32_t *adjc;         // k_leaf, one coloring: neighbour ids tagged with their colour, or null
     const int32_t *chunk_start;  // [hub_count+1] first chunk index of each hub
     const int32_t *off;
     const int32_t *adj;

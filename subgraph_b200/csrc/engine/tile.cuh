@@ -281,6 +281,19 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                 continue;
             }
             const int beg = __ldg(d.off + v), end = __ldg(d.off + v + 1);
+            if (d.adjc && nbc == 1) {
+                // colour-tagged neighbour ids: the colour comes with the id (top
+                // 4 bits), one load a neighbour
+                for (int e = beg; e < end; e += 8) {
+                    int cl[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) cl[u] = e + u < end ? (int)((uint32_t)__ldg(d.adjc + e + u) >> 28) : -1;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+                        if (cl[u] >= 0) cnt[cl[u] * RS] += T(1);
+                }
+                continue;
+            }
             const uint8_t *col = d.color + b;
             for (int e = beg; e < end; e += 8) {
                 int nb[8], cl[8];
@@ -949,7 +962,9 @@ __device__ __forceinline__ void hub_item(const HubArgs &h, int item, unsigned ch
         uint32_t *cnt = reinterpret_cast<uint32_t *>(smem_raw);
         for (int i = threadIdx.x; i < nk; i += NT) cnt[i] = 0;
         __syncthreads();
-        if (h.nb == 1 && h.cstride == 1) {
+        if (h.nb == 1 && h.adjc) {   // colour-tagged ids: one load a neighbour
+            for (int e = beg + (int)threadIdx.x; e < end; e += NT) atomicAdd(&cnt[(uint32_t)__ldg(h.adjc + e) >> 28], 1u);
+        } else if (h.nb == 1 && h.cstride == 1) {
             for (int e = beg + (int)threadIdx.x; e < end; e += NT) atomicAdd(&cnt[__ldg(h.color + __ldg(h.adj + e))], 1u);
         } else {
             for (int e = beg + (int)threadIdx.x; e < end; e += NT) {
