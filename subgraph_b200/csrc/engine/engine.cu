@@ -664,8 +664,15 @@ Status graph_finish(DeviceGraph &gr, const int32_t *deg, int32_t *d_old_off, int
         SG_CK(cudaMemcpyAsync(g->d_perm, perm.data(), sizeof(int32_t) * V, cudaMemcpyHostToDevice, st));
         SG_CK(cudaMemcpyAsync(g->d_iperm, iperm.data(), sizeof(int32_t) * V, cudaMemcpyHostToDevice, st));
     }
-    launch_remap(V, d_old_off, d_old_adj, g->d_off, g->d_iperm, g->d_perm, g->d_adj, st);
+    int32_t *d_bad = nullptr;
+    const int32_t none = INT32_MAX;
+    int32_t bad = none;
+    SG_CK(cudaMallocAsync(&d_bad, sizeof(int32_t), st));
+    SG_CK(cudaMemcpyAsync(d_bad, &none, sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    launch_remap(V, d_old_off, d_old_adj, g->d_off, g->d_iperm, g->d_perm, g->d_adj, d_bad, st);
     SG_CK(cudaGetLastError());
+    SG_CK(cudaMemcpyAsync(&bad, d_bad, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    cudaFreeAsync(d_bad, st);
     // coloring jump-ahead tables
     g->color_blocks = (V + kColorBlock - 1) / kColorBlock;
     std::vector<uint32_t> jump((size_t)std::max(g->color_blocks, 1) * 31), coef((size_t)31 * kColorBlock);
@@ -690,6 +697,7 @@ Status graph_finish(DeviceGraph &gr, const int32_t *deg, int32_t *d_old_off, int
     cudaFreeAsync(d_old_off, st);
     cudaFreeAsync(d_old_adj, st);
     SG_CK(cudaStreamSynchronize(st));
+    if (bad != none) return Status{1, "neighbour id out of range at entry " + std::to_string(bad)};
     return Status::ok();
 }
 
@@ -701,9 +709,7 @@ Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V,
     if (offsets[0] != 0 || offsets[V] != nnz) return Status{1, "offsets[0] must be 0 and offsets[V] must equal nnz"};
     for (int32_t v = 0; v < V; ++v)
         if (offsets[v + 1] < offsets[v]) return Status{1, "offsets are not monotone"};
-    // neighbour ids are range-checked on the host before the remap reads them
-    for (int64_t e = 0; e < nnz; ++e)
-        if ((uint32_t)neighbors[e] >= (uint32_t)V) return Status{1, "neighbour id out of range at entry " + std::to_string(e)};
+    // neighbour ids are range-checked by the remap kernel (graph_finish)
     std::unique_ptr<DeviceGraph> g;
     SG_CKS(new_device_graph(device, V, nnz, g));
     std::vector<int32_t> deg(V);

@@ -74,7 +74,7 @@ void launch_color(const ColorArgs &a, int ncolorings, cudaStream_t st)
 // ---------------------------------------------------------------------------
 __global__ void k_remap(int32_t V, const int32_t *__restrict__ old_off, const int32_t *__restrict__ old_adj,
                         const int32_t *__restrict__ new_off, const int32_t *__restrict__ iperm,
-                        const int32_t *__restrict__ perm, int32_t *__restrict__ new_adj)
+                        const int32_t *__restrict__ perm, int32_t *__restrict__ new_adj, int32_t *bad)
 {
     const int lane = threadIdx.x & 31;
     const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -82,16 +82,24 @@ __global__ void k_remap(int32_t V, const int32_t *__restrict__ old_off, const in
     for (int64_t v = w; v < V; v += nw) {
         const int32_t o = iperm[v];
         const int32_t b = old_off[o], e = old_off[o + 1], d = new_off[v];
-        for (int32_t i = b + lane; i < e; i += 32) new_adj[d + (i - b)] = perm[old_adj[i]];
+        for (int32_t i = b + lane; i < e; i += 32) {
+            const int32_t u = old_adj[i];
+            if ((uint32_t)u < (uint32_t)V) {
+                new_adj[d + (i - b)] = perm[u];
+            } else {
+                new_adj[d + (i - b)] = 0;
+                atomicMin(bad, i);
+            }
+        }
     }
 }
 
 void launch_remap(int32_t V, const int32_t *old_off, const int32_t *old_adj, const int32_t *new_off,
-                  const int32_t *iperm, const int32_t *perm, int32_t *new_adj, cudaStream_t st)
+                  const int32_t *iperm, const int32_t *perm, int32_t *new_adj, int32_t *bad, cudaStream_t st)
 {
     if (V == 0) return;
     int blocks = std::min<int64_t>(((int64_t)V * 32 + 255) / 256, 148 * 16);
-    k_remap<<<blocks, 256, 0, st>>>(V, old_off, old_adj, new_off, iperm, perm, new_adj);
+    k_remap<<<blocks, 256, 0, st>>>(V, old_off, old_adj, new_off, iperm, perm, new_adj, bad);
 }
 
 // ---------------------------------------------------------------------------

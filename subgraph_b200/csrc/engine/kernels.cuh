@@ -34,8 +34,11 @@ struct ColorArgs {
 void launch_color(const ColorArgs &a, int ncolorings, cudaStream_t st);
 // adjc[e] = adj[e] | color[adj[e]] << 28 (ids below 2^28, colors below 16)
 void launch_color_adj(const int32_t *adj, int64_t nnz, const uint8_t *color, int32_t *adjc, cudaStream_t st);
+// relabelled adjacency; a neighbour id outside [0, V) is not followed: the
+// first such entry's index is kept in *bad (atomicMin; the caller starts it
+// at INT32_MAX) and a 0 is written in its place
 void launch_remap(int32_t V, const int32_t *old_off, const int32_t *old_adj, const int32_t *new_off,
-                  const int32_t *iperm, const int32_t *perm, int32_t *new_adj, cudaStream_t st);
+                  const int32_t *iperm, const int32_t *perm, int32_t *new_adj, int32_t *bad, cudaStream_t st);
 
 struct FusedConfig {
     int tile_v;      // vertices per tile

@@ -96,3 +96,20 @@ def test_rmat_on_device_is_simple_symmetric_and_seeded():
     gh = sg.DeviceGraph(off, nbr)
     t = sg.Graph(*TEMPLATES["tree5"])
     assert np.array_equal(sg.count(g1, t, 2, 3, exact=True), sg.count(gh, t, 2, 3, exact=True))
+
+
+def test_out_of_range_neighbour_id_is_an_error():
+    """Neighbour ids are range-checked on the device while the graph is
+    relabelled: an id outside [0, V) fails the upload with the entry's index
+    (the first bad one) and leaves the device usable."""
+    off = np.array([0, 2, 3, 5, 6], np.int32)
+    nbr = np.array([1, 3, 0, 0, 7, 2], np.int32)   # entry 4 names vertex 7 of 4
+    with pytest.raises(sg.SGError, match="out of range at entry 4"):
+        sg.DeviceGraph(off, nbr)
+    nbr[4] = -1
+    with pytest.raises(sg.SGError, match="out of range at entry 4"):
+        sg.DeviceGraph(off, nbr)
+    nbr[4] = 3
+    g = sg.DeviceGraph(off, nbr)
+    t = sg.Graph(*TEMPLATES["p3"])
+    assert np.all(np.isfinite(sg.count(g, t, 2, 5)))
