@@ -10,7 +10,8 @@ tables, 16 colorings per step (coloring c seeded srand(7 + c)).
             launches on the library's stream, inputs resident in HBM.
   e2e       the same metric through the public C ABI per step: device graph
             built from pinned host CSC arrays (H2D copy inside the timed
-            region), all colorings counted, raw counts read back (D2H).
+            region), all colorings counted, raw counts read back (D2H);
+            W untimed warm-up steps first, as for value.
   roofline  the fused aggregation+eMA kernel: compulsory bytes per launch
             divided by its CUDA-event duration, against MEASURED_PEAKS.json.
   cpu_baseline  the reference's own CPU code (its CountMat::colorCounting,
@@ -507,6 +508,12 @@ def main():
         row = torch.from_numpy(csc.getIndexRow()).pin_memory()
         col_np, row_np = col.numpy(), row.numpy()
         h2d = 4 * (len(col_np) + len(row_np))
+        # untimed warm-up steps of this leg too: the first graph of the leg
+        # grows the device memory pool by its tables (the timed steps reuse it)
+        for s in range(args.warmup):
+            dg = sg.DeviceGraph(col_np, row_np, local)
+            sg.count(dg, tmpl, B, seeds(s), batch=args.batch, hub_threshold=args.hub, persistent=args.persistent)
+            del dg
         barrier()
         t0 = time.perf_counter()
         for s in range(args.steps):
