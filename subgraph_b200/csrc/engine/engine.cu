@@ -817,7 +817,8 @@ Status prepare(RunCtx &c, int ncolor_slots, int ncolorings_total)
     SG_CKS(growT(&w.partial, &w.partial_bytes, 8 * ((V / 8 + 2) * ncolor_slots), g.stream));
     SG_CKS(growT(&w.raw, &w.raw_bytes, 8 * (size_t)std::max(ncolorings_total, 1), g.stream));
     SG_CKS(growT(&w.windows, &w.windows_bytes, 4 * 31 * (size_t)std::max(ncolorings_total, 1), g.stream));
-    if (c.use_adjc) SG_CKS(growT(&w.adjc, &w.adjc_bytes, std::max<size_t>(16, 4 * (size_t)g.nnz), g.stream));
+    if (c.use_adjc)   // one colour-tagged adjacency per coloring of a slot (the interleaved group's)
+        SG_CKS(growT(&w.adjc, &w.adjc_bytes, std::max<size_t>(16, 4 * (size_t)g.nnz * c.lay), g.stream));
     if (c.mode == kModeOriginal) SG_CKS(growT(&w.orig_buf, &w.orig_buf_bytes, std::max<size_t>(16, 4 * V), g.stream));
     if (c.hubs.count > 0) {
         // a partial row holds the aux columns (or colour counts) of up to c.lay colorings
@@ -909,8 +910,9 @@ StageDesc make_stage(RunCtx &c, int slot, int s, double *root_vertex, int b0 = 0
     d.ublk_shape = d.blk_shape;
     d.ublk_nblocks = d.blk_nblocks;
     // the rooted form skips exact-zero products: FP32 reference arithmetic only
-    // (isPruned=0 tables may hold inf, where a skipped 0 * inf would be NaN)
-    if (!c.fp64 && c.blocked && c.rooted && c.mode == kModeReference && L == 1 && nb == 1 && c.tab->rblk[s]) {
+    // (isPruned=0 tables may hold inf, where a skipped 0 * inf would be NaN);
+    // one coloring a launch (of an interleaved group: a strided view of it)
+    if (!c.fp64 && c.blocked && c.rooted && c.mode == kModeReference && nb == 1 && c.tab->rblk[s]) {
         d.rblk = c.tab->rblk[s];
         d.rblk_shape = c.tab->rblk_shape[s];
         d.rblk_nblocks = c.tab->rblk_nblocks[s];
@@ -922,8 +924,8 @@ StageDesc make_stage(RunCtx &c, int slot, int s, double *root_vertex, int b0 = 0
         d.out_rank = c.tab->out_rank[s];
     }
     d.color = w.colors + (size_t)slot * g.V + b0;
-    if (c.use_adjc && L == 1) {
-        d.adjc = w.adjc + (size_t)slot * g.nnz;
+    if (c.use_adjc && nb == 1) {
+        d.adjc = w.adjc + ((size_t)slot * L + b0) * g.nnz;
         d.cmask = c.fp64 ? c.tab->cmask_f64[s] : c.tab->cmask_f32[s];
         d.cmask_stride = c.fp64 ? c.tab->cmf64_stride[s] : c.tab->cmf32_stride[s];
     }
@@ -1151,10 +1153,14 @@ Status launch_colors(RunCtx &c, int slot0, int first_coloring, int n, cudaStream
     a.vertex_stride = c.lay;
     launch_color(a, n, st);
     c.launches += 1;
-    if (c.use_adjc && c.lay == 1 && n == 1) {
-        launch_color_adj(c.g.d_adj, c.g.nnz, c.gs.ws.colors + (size_t)slot0 * c.g.V, c.gs.ws.adjc + (size_t)slot0 * c.g.nnz,
-                         st);
-        c.launches += 1;
+    if (c.use_adjc && (c.lay == 1 ? n == 1 : n <= c.lay)) {
+        // one colour-tagged adjacency per coloring: slot slot0's, or each of the
+        // interleaved group's (colours [V][lay])
+        for (int b = 0; b < (c.lay == 1 ? 1 : n); ++b) {
+            launch_color_adj(c.g.d_adj, c.g.nnz, c.gs.ws.colors + (size_t)slot0 * c.g.V + b, c.lay,
+                             c.gs.ws.adjc + ((size_t)slot0 * c.lay + b) * c.g.nnz, st);
+            c.launches += 1;
+        }
     }
     SG_CK(cudaGetLastError());
     return Status::ok();
@@ -1592,6 +1598,7 @@ Status count_grouped(RunCtx &c, const CountOptions &o, double *raw, CountStats *
         while (B > 1 && per * (size_t)B > (size_t)((double)(free_b + have) * 0.85)) B = (B + 1) / 2;
     }
     c.lay = B;
+    c.use_adjc = adjc_ok(g, p);
     SG_CKS(prepare(c, B, o.n_colorings));
     SG_CKS(upload_windows(c, o.seed_base, o.n_colorings));
     cudaEvent_t e0, e1;

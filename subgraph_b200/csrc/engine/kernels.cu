@@ -445,19 +445,20 @@ void launch_hub(const HubArgs &h, bool fp64, int sm_count, cudaStream_t st, int 
 // ---------------------------------------------------------------------------
 // Colored adjacency of one coloring: neighbour id | its color << 28.
 __global__ void k_color_adj(const int32_t *__restrict__ adj, int64_t nnz, const uint8_t *__restrict__ color,
-                            int32_t *__restrict__ adjc)
+                            int64_t cstride, int32_t *__restrict__ adjc)
 {
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x) {
         const int32_t u = adj[e];
-        adjc[e] = u | ((int32_t)color[u] << 28);
+        adjc[e] = u | ((int32_t)color[(size_t)u * cstride] << 28);
     }
 }
 
-void launch_color_adj(const int32_t *adj, int64_t nnz, const uint8_t *color, int32_t *adjc, cudaStream_t st)
+void launch_color_adj(const int32_t *adj, int64_t nnz, const uint8_t *color, int64_t cstride, int32_t *adjc,
+                      cudaStream_t st)
 {
     if (nnz <= 0) return;
     const int grid = (int)std::min<int64_t>((nnz + 255) / 256, 148 * 32);
-    k_color_adj<<<grid, 256, 0, st>>>(adj, nnz, color, adjc);
+    k_color_adj<<<grid, 256, 0, st>>>(adj, nnz, color, cstride, adjc);
 }
 
 // ---------------------------------------------------------------------------

@@ -32,8 +32,9 @@ struct ColorArgs {
 };
 
 void launch_color(const ColorArgs &a, int ncolorings, cudaStream_t st);
-// adjc[e] = adj[e] | color[adj[e]] << 28 (ids below 2^28, colors below 16)
-void launch_color_adj(const int32_t *adj, int64_t nnz, const uint8_t *color, int32_t *adjc, cudaStream_t st);
+// adjc[e] = adj[e] | color[adj[e] * cstride] << 28 (ids below 2^28, colors below 16)
+void launch_color_adj(const int32_t *adj, int64_t nnz, const uint8_t *color, int64_t cstride, int32_t *adjc,
+                      cudaStream_t st);
 // relabelled adjacency; a neighbour id outside [0, V) is not followed: the
 // first such entry's index is kept in *bad (atomicMin; the caller starts it
 // at INT32_MAX) and a 0 is written in its place

@@ -338,7 +338,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                         // read only when bit c_u of this vertex color's mask is set
                         // (other chunks: exact zeros, or columns whose products meet
                         // an exact zero); a skipped slot adds +0
-                        const uint16_t *cm = d.cmask + (size_t)__ldg(d.color + v) * d.cmask_stride;
+                        const uint16_t *cm = d.cmask + (size_t)__ldg(d.color + (size_t)v * d.cstride) * d.cmask_stride;
                         uint32_t msk[Q];
 #pragma unroll
                         for (int r = 0; r < Q; ++r) {
@@ -418,7 +418,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                 }
                 if (rooted) {
                     // only the columns lacking this vertex's color, at their rooted rank
-                    const uint32_t *ach = d.agg_chunk + (size_t)__ldg(d.color + v) * nchunk;
+                    const uint32_t *ach = d.agg_chunk + (size_t)__ldg(d.color + (size_t)v * d.cstride) * nchunk;
 #pragma unroll
                     for (int r = 0; r < Q; ++r) {
                         const int q = lane_g + G * r;
@@ -455,7 +455,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
             // the main columns holding this vertex's color, in rooted order
             for (int vi = warp; vi < tv; vi += NW) {
                 const T *row = mainp + (size_t)(v0 + vi) * d.main_pitch;
-                const int16_t *mf = d.main_full + (size_t)__ldg(d.color + v0 + vi) * d.r_Lm;
+                const int16_t *mf = d.main_full + (size_t)__ldg(d.color + (size_t)(v0 + vi) * d.cstride) * d.r_Lm;
                 for (int c = lane; c < d.r_Lm; c += 32) main_s[c * RS + vi] = ld_tab<COH>(row + __ldg(mf + c));
             }
         } else {
@@ -547,7 +547,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                     const int vj = fdiv(fd, idx), t = idx - vj * W;
                     T val = T(0);
                     if (t < d.L_s) {
-                        const int r = __ldg(d.out_rank + (size_t)__ldg(d.color + v0 + vj) * d.L_s + t);
+                        const int r = __ldg(d.out_rank + (size_t)__ldg(d.color + (size_t)(v0 + vj) * d.cstride) * d.L_s + t);
                         if (r >= 0) val = out_s[r * TVP + vj];
                     }
                     outp[(size_t)(v0 + vj) * P + t] = val;
