@@ -258,7 +258,12 @@ sg_status sg_plan_read(const char *path, sg_plan *out)
     SG_GUARD_END
 }
 
-void sg_plan_destroy(sg_plan p) { delete p; }
+void sg_plan_destroy(sg_plan p)
+{
+    if (!p) return;
+    sg::release_plan_tables(p->p.uid);
+    delete p;
+}
 
 sg_status sg_plan_info(sg_plan p, int32_t *k, int32_t *nsub, int32_t *scaled_sub, int64_t *arena_units)
 {

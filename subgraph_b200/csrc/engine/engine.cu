@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 
 #include <queue>
 
@@ -127,6 +128,9 @@ struct DevicePlanTables {
     // per sub with a non-leaf aux child: [k][chunks] masks for 32-byte chunks (8 FP32 / 4 FP64 columns)
     std::vector<uint16_t *> cmask_f32, cmask_f64;
     std::vector<int32_t> cmf32_stride, cmf64_stride;
+    // per sub with chunk masks: [k][chunks + 1] count and list of the chunks
+    // holding a set that lacks c (StageDesc::cact)
+    std::vector<uint16_t *> cact_f32, cact_f64;
 };
 
 // The work queue of one batch shape (plan, slots, mode, hubs), built once per
@@ -156,7 +160,6 @@ void free_batch(BatchPlan &b, cudaStream_t stream)
 
 struct GraphState {
     Workspace ws;
-    std::map<uint64_t, DevicePlanTables> plans;
     std::map<std::string, BatchPlan> batches; // batch shape -> work queue
     std::vector<cudaStream_t> streams;        // job streams (created on first use)
 };
@@ -171,6 +174,23 @@ std::string shape_key(const StageDesc &d, bool fp64, int hubs)
 
 std::map<const DeviceGraph *, GraphState> g_state;
 std::mutex g_state_mu;
+
+// Device copies of a plan's index tables.  They depend on the plan alone, so
+// one copy per (device, plan) serves every graph (a graph uploaded per call
+// finds them ready); release_plan_tables frees them with the plan.
+std::map<std::pair<int, uint64_t>, DevicePlanTables> g_plan_tables;   // guarded by g_state_mu
+
+void free_plan_tables(DevicePlanTables &t)
+{
+    auto drop = [](auto &v) {
+        for (auto *p : v)
+            if (p) cudaFree(p);
+    };
+    drop(t.split), drop(t.c2c), drop(t.rem), drop(t.aoff), drop(t.moff), drop(t.blk), drop(t.rblk);
+    drop(t.agg_chunk), drop(t.main_full), drop(t.out_rank), drop(t.cmask_f32), drop(t.cmask_f64);
+    drop(t.cact_f32), drop(t.cact_f64);
+    t = DevicePlanTables();
+}
 
 // Autotuner results, process-wide: a graph with the same signature (another
 // handle of the same CSC arrays, as the end-to-end path creates per call)
@@ -375,10 +395,21 @@ Status upload_chunk_masks(DeviceGraph &g, const Plan &p, int s, DevicePlanTables
             for (int j = 0; j < nch; ++j)
                 for (int t = j * w; t < std::min(a.L, j * w + w); ++t)
                     if (!(am[t] >> c & 1)) cm[(size_t)c * nch + j] |= (uint16_t)(am[t] & 0xffffu);
+        // a chunk is active for c when some set in it lacks c: its mask is then
+        // non-zero (every set holds a color)
+        std::vector<uint16_t> ca((size_t)k * (nch + 1), 0);
+        for (int c = 0; c < k; ++c) {
+            uint16_t *row = &ca[(size_t)c * (nch + 1)];
+            for (int j = 0; j < nch; ++j)
+                if (cm[(size_t)c * nch + j]) row[1 + row[0]++] = (uint16_t)j;
+        }
         uint16_t *&dst = w == 8 ? out.cmask_f32[s] : out.cmask_f64[s];
+        uint16_t *&dca = w == 8 ? out.cact_f32[s] : out.cact_f64[s];
         SG_CK(cudaMallocAsync(&dst, cm.size() * 2, g.stream));
+        SG_CK(cudaMallocAsync(&dca, ca.size() * 2, g.stream));
         SG_CK(cudaMemcpyAsync(dst, cm.data(), cm.size() * 2, cudaMemcpyHostToDevice, g.stream));
-        SG_CK(cudaStreamSynchronize(g.stream));   // `cm` is pageable and goes out of scope
+        SG_CK(cudaMemcpyAsync(dca, ca.data(), ca.size() * 2, cudaMemcpyHostToDevice, g.stream));
+        SG_CK(cudaStreamSynchronize(g.stream));   // `cm` and `ca` are pageable and go out of scope
         (w == 8 ? out.cmf32_stride : out.cmf64_stride)[s] = nch;
     }
     return Status::ok();
@@ -470,6 +501,8 @@ Status upload_plan(DeviceGraph &g, const Plan &p, DevicePlanTables &out)
     out.out_rank.assign(p.nsub(), nullptr);
     out.cmask_f32.assign(p.nsub(), nullptr);
     out.cmask_f64.assign(p.nsub(), nullptr);
+    out.cact_f32.assign(p.nsub(), nullptr);
+    out.cact_f64.assign(p.nsub(), nullptr);
     out.cmf32_stride.assign(p.nsub(), 0);
     out.cmf64_stride.assign(p.nsub(), 0);
     out.blk.assign(p.nsub(), nullptr);
@@ -581,20 +614,6 @@ DeviceGraph::~DeviceGraph()
                             (void *)w.chunk_start, (void *)w.root_vertex, (void *)w.adjc, (void *)w.orig_buf,
                             (void *)w.hub_ticket, (void *)w.tile_ticket})
                 if (p) cudaFreeAsync(p, stream);
-            for (auto &kv : it->second.plans) {
-                for (auto *p : kv.second.split) if (p) cudaFreeAsync(p, stream);
-                for (auto *p : kv.second.c2c) if (p) cudaFreeAsync(p, stream);
-                for (auto *p : kv.second.rem) if (p) cudaFreeAsync(p, stream);
-                for (auto *p : kv.second.aoff) if (p) cudaFreeAsync(p, stream);
-                for (auto *p : kv.second.blk) if (p) cudaFreeAsync(p, stream);
-                for (auto *p : kv.second.rblk) if (p) cudaFreeAsync(p, stream);
-                for (auto *p : kv.second.agg_chunk) if (p) cudaFreeAsync(p, stream);
-                for (auto *p : kv.second.main_full) if (p) cudaFreeAsync(p, stream);
-                for (auto *p : kv.second.out_rank) if (p) cudaFreeAsync(p, stream);
-                for (auto *p : kv.second.moff) if (p) cudaFreeAsync(p, stream);
-                for (auto *p : kv.second.cmask_f32) if (p) cudaFreeAsync(p, stream);
-                for (auto *p : kv.second.cmask_f64) if (p) cudaFreeAsync(p, stream);
-            }
             for (auto &kv : it->second.batches) free_batch(kv.second, stream);
             for (cudaStream_t js : it->second.streams) {
                 cudaStreamSynchronize(js);
@@ -630,40 +649,57 @@ Status new_device_graph(int device, int32_t V, int64_t nnz, std::unique_ptr<Devi
     return Status::ok();
 }
 
-// The common tail of every graph upload: the degree order (counting sort by
-// descending degree, stable in the id, on the V host degrees), the relabelled
-// adjacency (k_remap from the original-order device arrays, which this frees)
-// and the coloring jump-ahead tables.
-Status graph_finish(DeviceGraph &gr, const int32_t *deg, int32_t *d_old_off, int32_t *d_old_adj)
+// Jump-ahead polynomials of the coloring blocks: block b starts x^(341 + b *
+// kColorBlock) into the glibc stream.  They depend on nothing but b, so one
+// process-wide prefix serves every graph (extended when a larger graph needs
+// more blocks); the coefficients of x^t (t < kColorBlock) likewise.
+static std::mutex g_jump_mu;
+static std::vector<uint32_t> g_jump;   // [blocks][31]
+static Poly g_jump_next;               // the polynomial of the next block
+static std::vector<uint32_t> g_coef;   // [31][kColorBlock]
+
+static void color_tables(int blocks, std::vector<uint32_t> &jump, std::vector<uint32_t> &coef)
+{
+    std::lock_guard<std::mutex> lk(g_jump_mu);
+    if (g_coef.empty()) {
+        g_coef.assign((size_t)31 * kColorBlock, 0u);
+        Poly q(31, 0);
+        q[0] = 1;
+        for (int t = 0; t < kColorBlock; ++t) {
+            for (int i = 0; i < 31; ++i) g_coef[(size_t)i * kColorBlock + t] = q[i];
+            uint32_t top = q[30];
+            for (int j = 30; j > 0; --j) q[j] = q[j - 1];
+            q[0] = top;
+            q[28] += top;
+        }
+        g_jump_next = poly_xpow(341);
+    }
+    if ((int64_t)g_jump.size() < (int64_t)blocks * 31) {
+        const Poly step = poly_xpow(kColorBlock);
+        while ((int64_t)g_jump.size() < (int64_t)blocks * 31) {
+            g_jump.insert(g_jump.end(), g_jump_next.begin(), g_jump_next.end());
+            g_jump_next = poly_mulmod(g_jump_next, step);
+        }
+    }
+    jump.assign(g_jump.begin(), g_jump.begin() + (size_t)blocks * 31);
+    coef = g_coef;
+}
+
+// The common tail of every graph upload: the degree order (on the device),
+// the relabelled adjacency (k_remap from the original-order device arrays,
+// which this frees) and the coloring jump-ahead tables.
+Status graph_finish(DeviceGraph &gr, int32_t *d_old_off, int32_t *d_old_adj)
 {
     DeviceGraph *g = &gr;
     const int32_t V = g->V;
     const int64_t nnz = g->nnz;
-    int32_t maxd = 0;
-    for (int32_t v = 0; v < V; ++v) maxd = std::max(maxd, deg[v]);
-    g->max_degree = maxd;
-    std::vector<int64_t> bucket((size_t)maxd + 2, 0);
-    for (int32_t v = 0; v < V; ++v) bucket[(size_t)(maxd - deg[v]) + 1]++;
-    for (size_t i = 1; i < bucket.size(); ++i) bucket[i] += bucket[i - 1];
-    std::vector<int32_t> iperm(V), perm(V), noff((size_t)V + 1);
-    for (int32_t v = 0; v < V; ++v) iperm[bucket[(size_t)(maxd - deg[v])]++] = v;
-    g->h_degree.resize(V);
-    noff[0] = 0;
-    for (int32_t i = 0; i < V; ++i) {
-        perm[iperm[i]] = i;
-        g->h_degree[i] = deg[iperm[i]];
-        noff[i + 1] = noff[i] + g->h_degree[i];
-    }
     cudaStream_t st = g->stream;
     SG_CK(cudaMallocAsync(&g->d_off, sizeof(int32_t) * ((size_t)V + 1), st));
     SG_CK(cudaMallocAsync(&g->d_adj, sizeof(int32_t) * std::max<int64_t>(nnz, 1), st));
     SG_CK(cudaMallocAsync(&g->d_perm, sizeof(int32_t) * std::max<int32_t>(V, 1), st));
     SG_CK(cudaMallocAsync(&g->d_iperm, sizeof(int32_t) * std::max<int32_t>(V, 1), st));
-    SG_CK(cudaMemcpyAsync(g->d_off, noff.data(), sizeof(int32_t) * ((size_t)V + 1), cudaMemcpyHostToDevice, st));
-    if (V) {
-        SG_CK(cudaMemcpyAsync(g->d_perm, perm.data(), sizeof(int32_t) * V, cudaMemcpyHostToDevice, st));
-        SG_CK(cudaMemcpyAsync(g->d_iperm, iperm.data(), sizeof(int32_t) * V, cudaMemcpyHostToDevice, st));
-    }
+    SG_CKS(degree_order(V, d_old_off, g->d_iperm, g->d_perm, g->d_off, g->h_degree, st));
+    g->max_degree = V ? g->h_degree[0] : 0;
     int32_t *d_bad = nullptr;
     const int32_t none = INT32_MAX;
     int32_t bad = none;
@@ -675,21 +711,8 @@ Status graph_finish(DeviceGraph &gr, const int32_t *deg, int32_t *d_old_off, int
     cudaFreeAsync(d_bad, st);
     // coloring jump-ahead tables
     g->color_blocks = (V + kColorBlock - 1) / kColorBlock;
-    std::vector<uint32_t> jump((size_t)std::max(g->color_blocks, 1) * 31), coef((size_t)31 * kColorBlock);
-    Poly J = poly_xpow(341), step = poly_xpow(kColorBlock);
-    for (int b = 0; b < g->color_blocks; ++b) {
-        std::copy(J.begin(), J.end(), jump.begin() + (size_t)b * 31);
-        J = poly_mulmod(J, step);
-    }
-    Poly q(31, 0);
-    q[0] = 1;
-    for (int t = 0; t < kColorBlock; ++t) {
-        for (int i = 0; i < 31; ++i) coef[(size_t)i * kColorBlock + t] = q[i];
-        uint32_t top = q[30];
-        for (int j = 30; j > 0; --j) q[j] = q[j - 1];
-        q[0] = top;
-        q[28] += top;
-    }
+    std::vector<uint32_t> jump, coef;
+    color_tables(std::max(g->color_blocks, 1), jump, coef);
     SG_CK(cudaMallocAsync(&g->d_jump, jump.size() * 4, st));
     SG_CK(cudaMallocAsync(&g->d_coef, coef.size() * 4, st));
     SG_CK(cudaMemcpyAsync(g->d_jump, jump.data(), jump.size() * 4, cudaMemcpyHostToDevice, st));
@@ -699,6 +722,23 @@ Status graph_finish(DeviceGraph &gr, const int32_t *deg, int32_t *d_old_off, int
     SG_CK(cudaStreamSynchronize(st));
     if (bad != none) return Status{1, "neighbour id out of range at entry " + std::to_string(bad)};
     return Status::ok();
+}
+
+void release_plan_tables(uint64_t uid)
+{
+    std::lock_guard<std::mutex> lk(g_state_mu);
+    int prev = -1;
+    for (auto it = g_plan_tables.begin(); it != g_plan_tables.end();) {
+        if (it->first.second != uid) {
+            ++it;
+            continue;
+        }
+        if (prev < 0) cudaGetDevice(&prev);
+        cudaSetDevice(it->first.first);
+        free_plan_tables(it->second);   // cudaFree waits for the device's work
+        it = g_plan_tables.erase(it);
+    }
+    if (prev >= 0) cudaSetDevice(prev);
 }
 
 Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V, int64_t nnz, int device,
@@ -712,15 +752,13 @@ Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V,
     // neighbour ids are range-checked by the remap kernel (graph_finish)
     std::unique_ptr<DeviceGraph> g;
     SG_CKS(new_device_graph(device, V, nnz, g));
-    std::vector<int32_t> deg(V);
-    for (int32_t v = 0; v < V; ++v) deg[v] = offsets[v + 1] - offsets[v];
     int32_t *d_old_off = nullptr, *d_old_adj = nullptr;
     cudaStream_t st = g->stream;
     SG_CK(cudaMallocAsync(&d_old_off, sizeof(int32_t) * ((size_t)V + 1), st));
     SG_CK(cudaMallocAsync(&d_old_adj, sizeof(int32_t) * std::max<int64_t>(nnz, 1), st));
     SG_CK(cudaMemcpyAsync(d_old_off, offsets, sizeof(int32_t) * ((size_t)V + 1), cudaMemcpyHostToDevice, st));
     if (nnz) SG_CK(cudaMemcpyAsync(d_old_adj, neighbors, sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, st));
-    SG_CKS(graph_finish(*g, deg.data(), d_old_off, d_old_adj));
+    SG_CKS(graph_finish(*g, d_old_off, d_old_adj));
     out = std::move(g);
     return Status::ok();
 }
@@ -928,6 +966,8 @@ StageDesc make_stage(RunCtx &c, int slot, int s, double *root_vertex, int b0 = 0
         d.adjc = w.adjc + ((size_t)slot * L + b0) * g.nnz;
         d.cmask = c.fp64 ? c.tab->cmask_f64[s] : c.tab->cmask_f32[s];
         d.cmask_stride = c.fp64 ? c.tab->cmf64_stride[s] : c.tab->cmf32_stride[s];
+        d.ucact = c.fp64 ? c.tab->cact_f64[s] : c.tab->cact_f32[s];
+        d.cact_stride = d.cmask_stride + 1;
     }
     d.off = g.d_off;
     d.adj = g.d_adj;
@@ -1103,7 +1143,7 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
                 if (std::getenv("SG_TUNE_LOG"))
                     std::fprintf(stderr, "[sg tune] sub %d shape %s tile %d threads %d packed %d q %d group %d mask %d: %.3f ms\n",
                                  s, key.c_str(), cand.tile_v, cand.threads, cand.packed, dc.gather_q, dc.gather_group,
-                                 dc.cmask ? 1 : 0, ms);
+                                 dc.cact ? 2 : dc.cmask ? 1 : 0, ms);
             }
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);
@@ -1166,15 +1206,29 @@ Status launch_colors(RunCtx &c, int slot0, int first_coloring, int n, cudaStream
     return Status::ok();
 }
 
-Status make_ctx_tables(DeviceGraph &g, const Plan &p, GraphState &gs, DevicePlanTables *&tab)
+Status make_ctx_tables(DeviceGraph &g, const Plan &p, GraphState &, DevicePlanTables *&tab)
 {
-    auto it = gs.plans.find(p.uid);
-    if (it == gs.plans.end()) {
-        DevicePlanTables t;
-        SG_CKS(upload_plan(g, p, t));
-        it = gs.plans.emplace(p.uid, std::move(t)).first;
+    const std::pair<int, uint64_t> key{g.device, p.uid};
+    {
+        std::lock_guard<std::mutex> lk(g_state_mu);
+        auto it = g_plan_tables.find(key);
+        if (it != g_plan_tables.end()) {
+            tab = &it->second;
+            return Status::ok();
+        }
     }
-    tab = &it->second;
+    // uploaded on this graph's stream and synchronised (upload_plan), so any
+    // stream may read them afterwards
+    DevicePlanTables t;
+    Status st = upload_plan(g, p, t);
+    if (st.code) {
+        free_plan_tables(t);
+        return st;
+    }
+    std::lock_guard<std::mutex> lk(g_state_mu);
+    auto ins = g_plan_tables.try_emplace(key, std::move(t));
+    if (!ins.second) free_plan_tables(t);   // another thread uploaded them first
+    tab = &ins.first->second;
     return Status::ok();
 }
 

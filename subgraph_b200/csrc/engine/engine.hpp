@@ -79,13 +79,24 @@ struct CountStats {
 
 Status graph_create(const int32_t *offsets, const int32_t *neighbors, int32_t V, int64_t nnz, int device,
                     std::unique_ptr<DeviceGraph> &out);
+// Frees the device copies of a plan's index tables (kept per device and plan
+// for every graph that counts with it); called when the plan is destroyed.
+void release_plan_tables(uint64_t uid);
 
 // Pieces of a graph upload shared by the host-array and device-array paths:
 // a DeviceGraph with its stream, and the tail that orders the vertices by
-// degree (from the V host degrees), relabels the original-order device
-// adjacency (freed here) and builds the coloring tables.
+// degree (on the device, from the original-order offsets), relabels the
+// original-order device adjacency (both freed here) and builds the coloring
+// tables.
 Status new_device_graph(int device, int32_t V, int64_t nnz, std::unique_ptr<DeviceGraph> &out);
-Status graph_finish(DeviceGraph &g, const int32_t *deg, int32_t *d_old_off, int32_t *d_old_adj);
+Status graph_finish(DeviceGraph &g, int32_t *d_old_off, int32_t *d_old_adj);
+// The degree order of V vertices on the device (engine/input_gpu.cu): iperm =
+// the vertices by descending degree, ties by ascending id (a stable radix sort
+// on INT32_MAX - degree: the order of a stable counting sort by descending
+// degree), perm its inverse, new_off the exclusive sum of the ordered degrees;
+// the ordered degrees are copied to the host.
+Status degree_order(int32_t V, const int32_t *d_old_off, int32_t *d_iperm, int32_t *d_perm, int32_t *d_new_off,
+                    std::vector<int32_t> &h_degree, cudaStream_t st);
 
 // Input preparation on the GPU (engine/input_gpu.cu), each ending in a
 // DeviceGraph without a host copy of the adjacency:

@@ -62,10 +62,67 @@ __global__ void k_key_rows(int64_t n, const uint64_t *__restrict__ keys, int32_t
 
 int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
 
+__global__ void k_degree_keys(int32_t V, const int32_t *__restrict__ off, uint32_t *__restrict__ key,
+                              int32_t *__restrict__ ids)
+{
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x) {
+        key[v] = (uint32_t)(INT32_MAX - (off[v + 1] - off[v]));
+        ids[v] = (int32_t)v;
+    }
+}
+
+__global__ void k_degree_order(int32_t V, const uint32_t *__restrict__ key, const int32_t *__restrict__ iperm,
+                               int32_t *__restrict__ perm, int32_t *__restrict__ deg)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= V; i += (int64_t)gridDim.x * blockDim.x) {
+        if (i == V) {
+            deg[V] = 0;
+            continue;
+        }
+        perm[iperm[i]] = (int32_t)i;
+        deg[i] = INT32_MAX - (int32_t)key[i];
+    }
+}
+
+}  // namespace
+
+Status degree_order(int32_t V, const int32_t *d_old_off, int32_t *d_iperm, int32_t *d_perm, int32_t *d_new_off,
+                    std::vector<int32_t> &h_degree, cudaStream_t st)
+{
+    h_degree.assign(V, 0);
+    if (V == 0) {
+        IG_CK(cudaMemsetAsync(d_new_off, 0, sizeof(int32_t), st));
+        return Status::ok();
+    }
+    uint32_t *key = nullptr, *key_sorted = nullptr;
+    int32_t *ids = nullptr, *deg = nullptr;
+    IG_CK(cudaMallocAsync(&key, 4 * (size_t)V, st));
+    IG_CK(cudaMallocAsync(&key_sorted, 4 * (size_t)V, st));
+    IG_CK(cudaMallocAsync(&ids, 4 * (size_t)V, st));
+    IG_CK(cudaMallocAsync(&deg, 4 * ((size_t)V + 1), st));
+    k_degree_keys<<<grid_for(V), 256, 0, st>>>(V, d_old_off, key, ids);
+    IG_CK(cudaGetLastError());
+    size_t sort_bytes = 0, scan_bytes = 0;
+    IG_CK(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, key, key_sorted, ids, d_iperm, (int)V, 0, 32, st));
+    IG_CK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, deg, d_new_off, V + 1, st));
+    void *tmp = nullptr;
+    IG_CK(cudaMallocAsync(&tmp, std::max<size_t>(std::max(sort_bytes, scan_bytes), 16), st));
+    IG_CK(cub::DeviceRadixSort::SortPairs(tmp, sort_bytes, key, key_sorted, ids, d_iperm, (int)V, 0, 32, st));
+    k_degree_order<<<grid_for((int64_t)V + 1), 256, 0, st>>>(V, key_sorted, d_iperm, d_perm, deg);
+    IG_CK(cudaGetLastError());
+    IG_CK(cub::DeviceScan::ExclusiveSum(tmp, scan_bytes, deg, d_new_off, V + 1, st));
+    IG_CK(cudaMemcpyAsync(h_degree.data(), deg, 4 * (size_t)V, cudaMemcpyDeviceToHost, st));
+    for (void *p : {(void *)key, (void *)key_sorted, (void *)ids, (void *)deg, tmp}) cudaFreeAsync(p, st);
+    IG_CK(cudaStreamSynchronize(st));   // h_degree is pageable
+    return Status::ok();
+}
+
+namespace {
+
 // CSC of E host-or-device edges (device arrays here) into device offsets and
-// rows; the degrees land on the host for graph_finish.
+// rows.
 Status build_csc_device(int32_t V, const int32_t *d_src, const int32_t *d_dst, int64_t E, cudaStream_t st,
-                        int32_t *&d_off, int32_t *&d_rows, std::vector<int32_t> &deg)
+                        int32_t *&d_off, int32_t *&d_rows)
 {
     const int64_t nnz = 2 * E;
     if (nnz > 0x7fffffffLL) return Status{1, "too many edges"};
@@ -104,9 +161,6 @@ Status build_csc_device(int32_t V, const int32_t *d_src, const int32_t *d_dst, i
     void *scan_tmp = nullptr;
     IG_CK(cudaMallocAsync(&scan_tmp, std::max<size_t>(scan_bytes, 16), st));
     IG_CK(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, d_deg, d_off, V + 1, st));
-    deg.resize(V);
-    if (V) IG_CK(cudaMemcpyAsync(deg.data(), d_deg, 4 * (size_t)V, cudaMemcpyDeviceToHost, st));
-    IG_CK(cudaStreamSynchronize(st));
     for (void *p : {(void *)keys, (void *)sorted, (void *)d_deg, (void *)d_err, tmp, scan_tmp}) cudaFreeAsync(p, st);
     return Status::ok();
 }
@@ -115,14 +169,13 @@ Status finish_from_device_edges(int32_t V, int32_t *d_src, int32_t *d_dst, int64
 {
     cudaStream_t st = g->stream;
     int32_t *d_off = nullptr, *d_rows = nullptr;
-    std::vector<int32_t> deg;
-    Status s = build_csc_device(V, d_src, d_dst, E, st, d_off, d_rows, deg);
+    Status s = build_csc_device(V, d_src, d_dst, E, st, d_off, d_rows);
     cudaFreeAsync(d_src, st);
     cudaFreeAsync(d_dst, st);
     if (s.code) return s;
     g->V = V;
     g->nnz = 2 * E;
-    return graph_finish(*g, deg.data(), d_off, d_rows);
+    return graph_finish(*g, d_off, d_rows);
 }
 
 // ---------------------------------------------------------------------------

@@ -279,6 +279,12 @@ bool shape_fits(const StageDesc &d0, bool fp64, int tv, int nt, int packed, size
     return true;
 }
 
+bool flat_ok(const StageDesc &d, const TileShape &sh)
+{
+    return d.cmask && d.ucact && !d.aux_leaf && d.nb == 1 && sh.tile_v <= 32 && !sh.nomask &&
+           (d.main_leaf || (sh.packed == 2 && sh.rooted));
+}
+
 bool set_shape(StageDesc &d, bool fp64, const TileShape &sh)
 {
     size_t bytes;
@@ -292,6 +298,13 @@ bool set_shape(StageDesc &d, bool fp64, const TileShape &sh)
     d.smem = bytes;
     d.ntiles = (d.V + sh.tile_v - 1) / sh.tile_v;
     if (sh.nomask) d.cmask = nullptr;
+    d.cact = nullptr;
+    if (sh.flat) {
+        // only where every aggregate column read lacks the vertex's color (the
+        // rooted eMA, a one-hot main): the inactive chunks are then never read
+        if (!flat_ok(d, sh)) return false;
+        d.cact = d.ucact;
+    }
     return choose_gather(d, fp64, sh.q);
 }
 
@@ -337,6 +350,16 @@ std::vector<TileShape> candidate_shapes(const StageDesc &d, bool fp64)
                 if (q == e.gather_q) continue;
                 TileShape t = c;
                 t.q = q;
+                StageDesc f = d;
+                if (set_shape(f, fp64, t)) out.push_back(t);
+            }
+        }
+        // the flat aggregation over the active chunks, at each chunk count
+        if (flat_ok(d, c) && d.aux_cols >= 64) {
+            for (int q : {1, 2, 4}) {
+                TileShape t = c;
+                t.q = q;
+                t.flat = 1;
                 StageDesc f = d;
                 if (set_shape(f, fp64, t)) out.push_back(t);
             }

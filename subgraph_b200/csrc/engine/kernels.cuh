@@ -60,6 +60,7 @@ struct TileShape {
                      // nine in ten threads busy
     int nomask = 0;  // 1: read every column chunk (no chunk masks)
     int rooted = 0;  // register-blocked eMA in the rooted form (StageDesc::rooted)
+    int flat = 0;    // 1: flat aggregation over each vertex's active chunks (StageDesc::cact)
 };
 // Sets an explicit shape (the autotuner's candidates); false when it does not fit.
 bool set_shape(StageDesc &d, bool fp64, const TileShape &shape);

@@ -94,6 +94,14 @@ struct StageDesc {
     const int32_t *adjc;               // [nnz], or null (adj)
     const uint16_t *cmask;             // [k][cmask_stride] (with adjc, non-leaf aux), or null: every chunk read
     int32_t cmask_stride;
+    // Flat aggregation (with cmask, when only the aggregate columns lacking the
+    // vertex's color are read: rooted eMA or one-hot main): row c of cact is
+    // the count of the chunks that hold a set lacking c, then those chunks.
+    // The tile's (vertex, chunk group) pairs over those lists are spread over
+    // all threads instead of a fixed group of threads a vertex that also walks
+    // the chunks no output reads.  ucact: the table, cact: set when in use.
+    const uint16_t *cact, *ucact;      // [k][cact_stride]
+    int32_t cact_stride;
     const uint8_t *color;              // [V] internal order
     const int32_t *off;                // [V+1]
     const int32_t *adj;                // [nnz]

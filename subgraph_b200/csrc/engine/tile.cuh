@@ -313,8 +313,60 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
         const int nchunk = (d.aux_cols + CH - 1) / CH;
         const int rowc = d.aux_pitch / CH;
         const C *auxc = reinterpret_cast<const C *>(d.aux);
-        if (grp < ngrp) {
-            for (int vi = grp; vi < tv; vi += ngrp) {
+        // Work items: (vertex, chunk slots).  Grouped: the threads of group grp
+        // take vertices grp, grp + ngrp, ...; thread lane_g owns chunks
+        // lane_g + G*r.  Flat (d.cact): the tile's vertex v has
+        // ceil(nact(c(v)) / Q) items over its active chunks; item l owns active
+        // chunks l + n*r (n = the vertex's items), and the tile's items are
+        // spread over all threads (s_pre: their prefix sums over the vertices).
+        // A chunk slot at or past nchunk is idle.
+        // (not in the persistent kernel, COH, which never sets cact)
+        int *s_pre = nullptr;
+        if constexpr (!COH) {
+            __shared__ int s_pre_buf[33];
+            s_pre = s_pre_buf;
+        }
+        const bool flat = !COH && d.cact != nullptr;
+        if (flat) {
+            if (warp == 0) {
+                int n = 0;
+                if (lane < tv) {
+                    const int cv = __ldg(d.color + (size_t)(v0 + lane) * d.cstride);
+                    n = ((int)__ldg(d.cact + (size_t)cv * d.cact_stride) + Q - 1) / Q;
+                }
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, n, o);
+                    if (lane >= o) n += y;
+                }
+                if (lane < tv) s_pre[lane + 1] = n;
+                if (lane == 0) s_pre[0] = 0;
+            }
+            __syncthreads();
+        }
+        const int w_end = flat ? s_pre[tv] : tv;
+        const int w_step = flat ? NT : ngrp;
+        for (int wi = flat ? tid : (grp < ngrp ? grp : tv); wi < w_end; wi += w_step) {
+            int vi, qv[Q];
+            if (flat) {
+                int lo = 0, hi = tv;   // s_pre[lo] <= wi < s_pre[hi]
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (s_pre[mid] <= wi) lo = mid;
+                    else hi = mid;
+                }
+                vi = lo;
+                const int l = wi - s_pre[vi], n = s_pre[vi + 1] - s_pre[vi];
+                const uint16_t *ca = d.cact + (size_t)__ldg(d.color + (size_t)(v0 + vi) * d.cstride) * d.cact_stride;
+                const int nact = __ldg(ca);
+#pragma unroll
+                for (int r = 0; r < Q; ++r) qv[r] = l + n * r < nact ? (int)__ldg(ca + 1 + l + n * r) : nchunk;
+            } else {
+                vi = wi;
+#pragma unroll
+                for (int r = 0; r < Q; ++r) qv[r] = lane_g + G * r;
+            }
+            {
                 const int v = v0 + vi;
                 C acc[Q];
                 if (v < d.hub_count) {
@@ -323,7 +375,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                     const int c0 = __ldg(d.hub_chunk_start + v), c1 = __ldg(d.hub_chunk_start + v + 1);
 #pragma unroll
                     for (int r = 0; r < Q; ++r) {
-                        const int q = lane_g + G * r;
+                        const int q = qv[r];
                         acc[r] = CT::zero();
                         if (q < nchunk)
                             for (int ch = c0; ch < c1; ++ch) CT::add(acc[r], ld_tab<COH>(p + (size_t)ch * prc + q));
@@ -342,7 +394,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                         uint32_t msk[Q];
 #pragma unroll
                         for (int r = 0; r < Q; ++r) {
-                            const int q = lane_g + G * r;
+                            const int q = qv[r];
                             msk[r] = q < nchunk ? (uint32_t)__ldg(cm + q) : 0u;
                         }
                         for (int e = beg; e < end; e += U) {
@@ -354,7 +406,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                             for (int u = 0; u < U; ++u)
 #pragma unroll
                                 for (int r = 0; r < Q; ++r) {
-                                    const int q = lane_g + G * r;
+                                    const int q = qv[r];
                                     x[u][r] = (e + u < end && ((msk[r] >> ((uint32_t)nw[u] >> 28)) & 1u))
                                                   ? ld_tab<COH>(auxc + (size_t)(nw[u] & 0x0fffffff) * rowc + q)
                                                   : CT::zero();
@@ -364,7 +416,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
 #pragma unroll
                                 for (int r = 0; r < Q; ++r) CT::add(acc[r], x[u][r]);
                         }
-                    } else if (lane_g + G * (Q - 1) < nchunk) {
+                    } else if (qv[Q - 1] < nchunk) {
                         // every slot of this thread lies in the row: full batches of U
                         // neighbours without predicates, then the remaining ones singly
                         // (the same neighbour order, so the same sums)
@@ -405,7 +457,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                             for (int u = 0; u < U; ++u)
 #pragma unroll
                                 for (int r = 0; r < Q; ++r) {
-                                    const int q = lane_g + G * r;
+                                    const int q = qv[r];
                                     x[u][r] = (q < nchunk && nb[u] >= 0) ? ld_tab<COH>(auxc + (size_t)nb[u] * rowc + q)
                                                                          : CT::zero();
                                 }
@@ -421,7 +473,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                     const uint32_t *ach = d.agg_chunk + (size_t)__ldg(d.color + (size_t)v * d.cstride) * nchunk;
 #pragma unroll
                     for (int r = 0; r < Q; ++r) {
-                        const int q = lane_g + G * r;
+                        const int q = qv[r];
                         if (q < nchunk) {
                             const uint32_t w = __ldg(ach + q);
                             const uint32_t lack = w >> 16;
@@ -435,7 +487,7 @@ __device__ __forceinline__ void fused_tile(const StageDesc &d, int tile, unsigne
                 } else {
 #pragma unroll
                     for (int r = 0; r < Q; ++r) {
-                        const int q = lane_g + G * r;
+                        const int q = qv[r];
                         if (q < nchunk) {
 #pragma unroll
                             for (int i = 0; i < CH; ++i) {
