@@ -55,7 +55,7 @@ WORKLOADS = {
                               # DRAM bytes (read + write) of one launch of the dominant stage (sub 10),
                               # measured by ncu on the same kernel at R-MAT scale 18 (tree12_rmat18_ef8)
                               # and scaled by the ratio of its algorithmic bytes (x4.0006)
-                              dominant_traffic=dict(sub=10, bytes=2.4889e9 * 4.0006,
+                              dominant_traffic=dict(sub=10, bytes=2.5298e9 * 4.0006,
                                                     source="ncu dram__bytes_read.sum + dram__bytes_write.sum of "
                                                            "the sub-10 launch at R-MAT scale 18, x4.0006 to scale 20")),
     "p3_rmat16_ef16": dict(scale=16, ef=16, template="p3", per_step=1, seed=7),

@@ -183,6 +183,9 @@ typedef struct {
     int32_t no_rooted;      /* 1: no rooted form of the register-blocked eMA (a vertex of color c
                                computes only the outputs and products whose sets hold c, over
                                the other k-1 colors); the two give identical values */
+    int32_t no_flat;        /* 1: no flat aggregation (the tile's vertices each take a fixed group
+                               of threads, which also walk the column chunks no output of the
+                               vertex reads); the two give identical values */
 } sg_count_opts;
 
 typedef struct {

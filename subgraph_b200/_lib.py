@@ -53,7 +53,8 @@ class CountOpts(ctypes.Structure):
                 ("batch", ctypes.c_int32), ("hub_threshold", ctypes.c_int32), ("profile", ctypes.c_int32),
                 ("no_autotune", ctypes.c_int32), ("exact", ctypes.c_int32), ("wait_limit_ms", ctypes.c_int32),
                 ("no_blocked", ctypes.c_int32),
-                ("persistent", ctypes.c_int32), ("no_rooted", ctypes.c_int32)]
+                ("persistent", ctypes.c_int32), ("no_rooted", ctypes.c_int32),
+                ("no_flat", ctypes.c_int32)]
 
 
 class CountStats(ctypes.Structure):

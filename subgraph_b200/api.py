@@ -449,7 +449,8 @@ class IndexSys:
 def count(graph: DeviceGraph, template: Graph, n_colorings: int = 1, seed_base: int = 0,
           mode: int = MODE_REFERENCE, batch: int = 0, hub_threshold: int = 1024,
           return_stats: bool = False, profile: bool = False, autotune: bool = True, exact: bool = False,
-          wait_limit_ms: int = 0, blocked: bool = True, persistent: bool = False, rooted: bool = True):
+          wait_limit_ms: int = 0, blocked: bool = True, persistent: bool = False, rooted: bool = True,
+          flat: bool = True):
     """Raw colorful counts of n_colorings colorings (coloring c uses srand(seed_base + c))."""
     o = CountOpts()
     lib().sg_count_opts_default(ctypes.byref(o))
@@ -464,6 +465,7 @@ def count(graph: DeviceGraph, template: Graph, n_colorings: int = 1, seed_base: 
     o.wait_limit_ms = wait_limit_ms
     o.no_blocked = 0 if blocked else 1
     o.no_rooted = 0 if rooted else 1
+    o.no_flat = 0 if flat else 1
     o.persistent = 1 if persistent else 0
     raw = np.zeros(n_colorings, np.float64)
     st = CountStats()

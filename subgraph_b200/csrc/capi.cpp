@@ -422,6 +422,7 @@ sg::CountOptions count_options(const sg_count_opts *o)
     co.wait_limit_ms = o->wait_limit_ms;
     co.blocked = o->no_blocked ? 0 : 1;
     co.rooted = o->no_rooted ? 0 : 1;
+    co.flat = o->no_flat ? 0 : 1;
     co.persistent = o->persistent;
     return co;
 }
@@ -486,6 +487,7 @@ sg_status sg_count_jobs(sg_graph g, int32_t n_jobs, const sg_plan *plans, const 
     co.batch = o->batch;
     co.blocked = o->no_blocked ? 0 : 1;
     co.rooted = o->no_rooted ? 0 : 1;
+    co.flat = o->no_flat ? 0 : 1;
     sg::CountStats cs;
     sg_status st = from(sg::count_jobs(*g->g, ps, seeds, co, raw, job_ms, &cs));
     if (st) return st;

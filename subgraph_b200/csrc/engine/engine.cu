@@ -783,6 +783,7 @@ struct RunCtx {
     bool autotune = false;
     bool blocked = true;     // register-blocked eMA allowed
     bool rooted = true;      // its rooted form allowed
+    bool flat = true;        // the flat aggregation allowed
     int lay = 1;             // colorings interleaved per table row (grouped batched form)
     size_t arena_base = 0;   // byte offset of this context's tables in the arena (job queues)
     bool exact = false;      // no fused products (packed eMA), no hub chunks
@@ -966,7 +967,7 @@ StageDesc make_stage(RunCtx &c, int slot, int s, double *root_vertex, int b0 = 0
         d.adjc = w.adjc + ((size_t)slot * L + b0) * g.nnz;
         d.cmask = c.fp64 ? c.tab->cmask_f64[s] : c.tab->cmask_f32[s];
         d.cmask_stride = c.fp64 ? c.tab->cmf64_stride[s] : c.tab->cmf32_stride[s];
-        d.ucact = c.fp64 ? c.tab->cact_f64[s] : c.tab->cact_f32[s];
+        d.ucact = !c.flat ? nullptr : c.fp64 ? c.tab->cact_f64[s] : c.tab->cact_f32[s];
         d.cact_stride = d.cmask_stride + 1;
     }
     d.off = g.d_off;
@@ -1712,6 +1713,7 @@ Status count(DeviceGraph &g, const Plan &p, const CountOptions &o, double *raw, 
     c.autotune = o.autotune != 0;
     c.blocked = o.blocked != 0;
     c.rooted = o.rooted != 0;
+    c.flat = o.flat != 0;
     // mode 2 carries its aggregation buffer from one coloring to the next, so
     // its colorings always run one after another (the plain form)
     if (o.batch > 0 && o.mode != kModeOriginal)
@@ -2098,6 +2100,7 @@ Status count_jobs_streams(DeviceGraph &g, const std::vector<const Plan *> &plans
         c.autotune = o.autotune != 0;
         c.blocked = o.blocked != 0;
         c.rooted = o.rooted != 0;
+        c.flat = o.flat != 0;
         c.use_adjc = adjc_ok(g, p);
         max_arena = std::max(max_arena, (size_t)p.arena_units * V * es);
         hub_pitch = std::max<int32_t>(hub_pitch, (int32_t)round_up(p.k, 8));

@@ -58,6 +58,7 @@ struct CountOptions {
     int32_t test_unsatisfiable_wait = 0;   // test hook: the first fused stage waits on a counter nothing sets
     int32_t blocked = 1;            // register-blocked eMA where a stage has one (same values)
     int32_t rooted = 1;             // its rooted form where a stage has one (same values)
+    int32_t flat = 1;               // flat aggregation over the active chunks where it applies (same values)
     float *orig_state = nullptr;    // mode 2: host [V] aggregation buffer (original vertex order is not
                                     // needed: internal order, opaque to the caller) carried in and out;
                                     // null: start from zeros

@@ -400,6 +400,15 @@ bool plan_fused(StageDesc &d, bool fp64, int sm_count, FusedConfig &cfg)
             if (shape_fits(d, fp64, tv, 512, 0, limits[li], bytes, oc)) { ok = set_shape(d, fp64, TileShape{tv, 512, 0}); break; }
         }
     if (!ok) return false;
+    // the flat aggregation where the chosen shape allows it (the autotuner
+    // times both)
+    if (d.ucact) {
+        TileShape t{d.tile_v, d.nthreads, d.packed};
+        t.rooted = d.rooted;
+        t.flat = 1;
+        StageDesc f = d;
+        if (flat_ok(f, t) && set_shape(f, fp64, t)) d = f;
+    }
     cfg.tile_v = d.tile_v;
     cfg.q = d.gather_q;
     cfg.smem = d.smem;

@@ -82,3 +82,31 @@ def test_rooted_form_equals_full_form(golden):
                 # per-vertex values are identical; only the FP64 sum of tile
                 # partials may differ in order if the two runs tile the root differently
                 assert all(rel(x, y) <= 1e-12 for x, y in zip(a, b)), (gname, n, edges, hub, a, b)
+
+
+def test_flat_aggregation_equals_grouped(golden):
+    """The flat aggregation (the tile's (vertex, chunk group) items spread over
+    all threads, each vertex walking only the column chunks that hold a set
+    lacking its color) gives the grouped form's values bit for bit: untuned
+    shapes (flat by default where it applies), FP32 exact and fast paths and
+    FP64 tables, with and without hub rows; exact FP32 also against the
+    reference's raw counts."""
+    rng = random.Random(41)
+    trees = [TEMPLATES["tree12"], TEMPLATES["spider7"], TEMPLATES["tree5"]]
+    trees += [(n, prufer_tree(n, rng)) for n in [rng.randint(5, 12) for _ in range(6)]]
+    for gname in ("rmat10", "rmat12"):
+        _, _, _, col, row = golden.graph(gname)
+        g = sg.DeviceGraph(col, row)
+        for n, edges in trees:
+            t = sg.Graph(n, edges)
+            for hub in (0, 16):
+                for kw in (dict(exact=True), dict(exact=False), dict(mode=sg.MODE_FP64)):
+                    a = sg.count(g, t, 2, 31, autotune=False, hub_threshold=hub, **kw)
+                    b = sg.count(g, t, 2, 31, autotune=False, hub_threshold=hub, flat=False, **kw)
+                    assert np.array_equal(a, b), (gname, n, edges, hub, kw, a, b)
+    for c in [c for c in golden.cases if c.template in ("tree12", "spider7")]:
+        _, _, _, col, row = golden.graph(c.graph)
+        g = sg.DeviceGraph(col, row)
+        a = sg.count(g, sg.Graph(c.n, c.edges), c.ncol, c.seed, exact=True, autotune=False)
+        for i in range(c.ncol):
+            assert rel(a[i], c.raw[i]) <= 1e-12, (c.key, i)
