@@ -131,6 +131,10 @@ struct DevicePlanTables {
     // per sub with chunk masks: [k][chunks + 1] count and list of the chunks
     // holding a set that lacks c (StageDesc::cact)
     std::vector<uint16_t *> cact_f32, cact_f64;
+    // per sub with chunk masks: [k][32-column groups] masks of the exact-order
+    // hub items (HubArgs::gmask)
+    std::vector<uint16_t *> hub_gmask;
+    std::vector<int32_t> hgm_stride;
 };
 
 // The work queue of one batch shape (plan, slots, mode, hubs), built once per
@@ -188,7 +192,7 @@ void free_plan_tables(DevicePlanTables &t)
     };
     drop(t.split), drop(t.c2c), drop(t.rem), drop(t.aoff), drop(t.moff), drop(t.blk), drop(t.rblk);
     drop(t.agg_chunk), drop(t.main_full), drop(t.out_rank), drop(t.cmask_f32), drop(t.cmask_f64);
-    drop(t.cact_f32), drop(t.cact_f64);
+    drop(t.cact_f32), drop(t.cact_f64), drop(t.hub_gmask);
     t = DevicePlanTables();
 }
 
@@ -388,6 +392,19 @@ Status upload_chunk_masks(DeviceGraph &g, const Plan &p, int s, DevicePlanTables
         for (int i = 0; i < na; ++i) m |= 1u << el[i];
         am[t] = m;
     }
+    {
+        // the exact-order hub items' 32-column groups (FP32 and FP64 alike)
+        const int ng = (a.L + 31) / 32;
+        std::vector<uint16_t> gm((size_t)k * ng, 0);
+        for (int c = 0; c < k; ++c)
+            for (int j = 0; j < ng; ++j)
+                for (int t = j * 32; t < std::min(a.L, j * 32 + 32); ++t)
+                    if (!(am[t] >> c & 1)) gm[(size_t)c * ng + j] |= (uint16_t)(am[t] & 0xffffu);
+        SG_CK(cudaMallocAsync(&out.hub_gmask[s], gm.size() * 2, g.stream));
+        SG_CK(cudaMemcpyAsync(out.hub_gmask[s], gm.data(), gm.size() * 2, cudaMemcpyHostToDevice, g.stream));
+        SG_CK(cudaStreamSynchronize(g.stream));   // `gm` is pageable and goes out of scope
+        out.hgm_stride[s] = ng;
+    }
     for (int w : {8, 4}) {   // chunk columns: FP32, FP64
         const int nch = (a.L + w - 1) / w;
         std::vector<uint16_t> cm((size_t)k * nch, 0);
@@ -503,6 +520,8 @@ Status upload_plan(DeviceGraph &g, const Plan &p, DevicePlanTables &out)
     out.cmask_f64.assign(p.nsub(), nullptr);
     out.cact_f32.assign(p.nsub(), nullptr);
     out.cact_f64.assign(p.nsub(), nullptr);
+    out.hub_gmask.assign(p.nsub(), nullptr);
+    out.hgm_stride.assign(p.nsub(), 0);
     out.cmf32_stride.assign(p.nsub(), 0);
     out.cmf64_stride.assign(p.nsub(), 0);
     out.blk.assign(p.nsub(), nullptr);
@@ -979,7 +998,7 @@ StageDesc make_stage(RunCtx &c, int slot, int s, double *root_vertex, int b0 = 0
 
 // The hub aggregation feeding stage d, writing its partial rows to `partial`;
 // also points d at those rows.
-HubArgs make_hub(RunCtx &c, StageDesc &d, void *partial)
+HubArgs make_hub(RunCtx &c, StageDesc &d, void *partial, int s)
 {
     DeviceGraph &g = c.g;
     HubArgs h{};
@@ -1001,6 +1020,13 @@ HubArgs make_hub(RunCtx &c, StageDesc &d, void *partial)
     h.aux = d.aux;
     h.partial = partial;
     h.ticket = c.gs.ws.hub_ticket ? c.gs.ws.hub_ticket + c.ticket : nullptr;
+    // skipped slices need the exact-zero structure of the reference and FP64
+    // tables (isPruned=0 runs no hub kernel) and the colour-tagged ids
+    if (h.exact_order && !h.k_leaf && d.adjc && d.nb == 1 && c.tab->hub_gmask[s] &&
+        (c.mode == kModeReference || c.mode == kModeFP64)) {
+        h.gmask = c.tab->hub_gmask[s];
+        h.gmask_stride = c.tab->hgm_stride[s];
+    }
     d.hub_count = c.hubs.count;
     d.hub_pitch = c.hub_pitch;
     d.hub_chunk_start = c.gs.ws.chunk_start;
@@ -1052,7 +1078,7 @@ Status run_stage(RunCtx &c, int slot, int s, double *root_vertex, cudaStream_t s
     DeviceGraph &g = c.g;
     StageDesc d = make_stage(c, slot, s, root_vertex, b0, nb);
     if (c.hubs.count > 0) {
-        HubArgs h = make_hub(c, d, c.hub_region ? c.hub_region : c.gs.ws.hub_partial);
+        HubArgs h = make_hub(c, d, c.hub_region ? c.hub_region : c.gs.ws.hub_partial, s);
         int variant = 0;
         if (h.exact_order && !h.k_leaf) {
             // the exact-order hub kernel's (threads, ring depth) pair: timed once per
@@ -1365,7 +1391,7 @@ Status add_queue_stage(RunCtx &c, int slot, int s, void *hub_region, QueueSlot &
     if (c.hubs.count > 0) {
         BatchStage hs{};
         hs.kind = kStageHub;
-        hs.h = make_hub(c, d, hub_region);
+        hs.h = make_hub(c, d, hub_region, s);
         hs.first_item = item;
         hs.nitems = (c.hubs.total_chunks + kHubItemChunks - 1) / kHubItemChunks;
         if (p.subs[sub.aux].size > 1) hs.deps[hs.ndeps++] = q.fused[sub.aux];

@@ -119,8 +119,8 @@ struct HubArgs {
     int32_t k_leaf;              // > 0: the aux child is one-hot, count colors (k) of nb colorings
     int32_t nb, cstride;         // k_leaf: colorings, color layout (color[v * cstride + b])
     int32_t total_chunks;
-    const uint8_t *color;        // [V] internal order (k_leaf only)
-    const int32_t *adjc;         // k_leaf, one coloring: neighbour ids tagged with their colour, or null
+    const uint8_t *color;        // [V] internal order (k_leaf, gmask)
+    const int32_t *adjc;         // one coloring: neighbour ids tagged with their colour, or null (k_leaf, gmask)
     const int32_t *chunk_start;  // [hub_count+1] first chunk index of each hub
     const int32_t *off;
     const int32_t *adj;
@@ -131,6 +131,14 @@ struct HubArgs {
     // neighbour list in order -- the reference's summation order
     int32_t exact_order;
     int32_t *ticket;             // exact order: the next item to take (zeroed before each launch)
+    // exact order, colour-tagged ids (adjc): gmask[c][g] has bit c_u set when
+    // the 32-column group g holds a set with c_u and without c.  A hub of
+    // colour c copies group g of a neighbour of colour c_u only then (else a
+    // zero slice): the neighbour's other entries of the group are exact zeros
+    // or lie in columns holding c, which no reader of the hub row uses (they
+    // meet main entries that are exact zeros, or no output).  Null: every slice.
+    const uint16_t *gmask;
+    int32_t gmask_stride;
 };
 
 // ---------------------------------------------------------------------------

@@ -871,7 +871,12 @@ __device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, unsig
     const uint64_t src0 = reinterpret_cast<uint64_t>(reinterpret_cast<const T *>(h.aux) + c0 + (lr_in ? lr * PC : 0));
     const uint32_t row_bytes = (uint32_t)h.aux_pitch * (uint32_t)sizeof(T);
     const uint32_t dst0 = ring_s + (uint32_t)((ln * RPL * SS + lr * PC) * sizeof(T));
-    const int32_t *adj_v = h.adj + beg;
+    // with group masks the ids carry their colour (top 4 bits) and a
+    // neighbour's slice is copied only when this group needs its colour
+    const bool masked = h.gmask != nullptr;
+    const int32_t *adj_v = (masked ? h.adjc : h.adj) + beg;
+    const uint32_t gm =
+        masked ? (uint32_t)__ldg(h.gmask + (size_t)__ldg(h.color + (size_t)v * h.cstride) * h.gmask_stride + grp) : ~0u;
     // ids lane, lane + 32, ... of batch j into the id slot at byte offset
     // `slot_b` (zero past the list: a valid row that is never added)
     auto fetch_ids = [&](int j, uint32_t slot_b) {
@@ -882,19 +887,25 @@ __device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, unsig
             cp_async4_zs(ids_s + slot_b + (i * 32 + lane) * 4, adj_v + (in ? e : 0), in ? 4u : 0u);
         }
     };
-    // A batch's copy plan for this lane: the source of each of its RPL pieces.
+    // A batch's copy plan for this lane: the source of each of its RPL pieces
+    // and, bit k of `need`, whether piece k is read (else zero-filled).
     uint64_t src[RPL];
+    uint32_t need = 0;
     auto plan = [&](uint32_t is_b) {
         const int4 *bid = reinterpret_cast<const int4 *>(ids + is_b / 4 + ln * RPL);
+        need = 0;
 #pragma unroll
         for (int q = 0; q < RPL / 4; ++q) {
             const int4 t = bid[q];
-            src[4 * q] = src0 + (uint64_t)(uint32_t)t.x * row_bytes;
-            src[4 * q + 1] = src0 + (uint64_t)(uint32_t)t.y * row_bytes;
-            src[4 * q + 2] = src0 + (uint64_t)(uint32_t)t.z * row_bytes;
-            src[4 * q + 3] = src0 + (uint64_t)(uint32_t)t.w * row_bytes;
+            const uint32_t w[4] = {(uint32_t)t.x, (uint32_t)t.y, (uint32_t)t.z, (uint32_t)t.w};
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                src[4 * q + i] = src0 + (uint64_t)(w[i] & 0x0fffffffu) * row_bytes;
+                need |= (gm >> (w[i] >> 28) & 1u) << (4 * q + i);
+            }
         }
     };
+    auto piece = [&](int k) -> uint32_t { return (need >> k & 1u) * 16u; };
     // batch b's copies into the ring slot at byte offset ts_b: every row of a
     // full batch, the rows inside the list of the last one, none past it
     auto copy = [&](int b, uint32_t ts_b) {
@@ -902,12 +913,13 @@ __device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, unsig
         const uint32_t d = dst0 + ts_b;
         if (left >= BR) {
 #pragma unroll
-            for (int k = 0; k < RPL; ++k) cp_async16_s(d + (uint32_t)(k * SS * sizeof(T)), reinterpret_cast<const void *>(src[k]));
+            for (int k = 0; k < RPL; ++k)
+                cp_async16_zs(d + (uint32_t)(k * SS * sizeof(T)), reinterpret_cast<const void *>(src[k]), piece(k));
         } else if (left > 0) {
 #pragma unroll
             for (int k = 0; k < RPL; ++k)
                 if (ln * RPL + k < left)
-                    cp_async16_s(d + (uint32_t)(k * SS * sizeof(T)), reinterpret_cast<const void *>(src[k]));
+                    cp_async16_zs(d + (uint32_t)(k * SS * sizeof(T)), reinterpret_cast<const void *>(src[k]), piece(k));
         }
     };
     auto load = [&](T(&x)[BR], uint32_t ts_b) {
@@ -943,7 +955,7 @@ __device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, unsig
         if (!tail) {
 #pragma unroll
             for (int k = 0; k < RPL; ++k)
-                cp_async16_s(dst0 + ts_b + (uint32_t)(k * SS * sizeof(T)), reinterpret_cast<const void *>(src[k]));
+                cp_async16_zs(dst0 + ts_b + (uint32_t)(k * SS * sizeof(T)), reinterpret_cast<const void *>(src[k]), piece(k));
         } else {
             copy(b + NSLOT - 1, ts_b);
         }
