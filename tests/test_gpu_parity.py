@@ -264,6 +264,30 @@ def test_deterministic_runs():
     assert np.array_equal(a, b)
 
 
+def test_hub_rows_equal_no_hubs(golden):
+    """Exact mode: the hub kernel's rows (each column summed over the whole
+    neighbour list in order, a neighbour's slice copied only where the hub's
+    colour and the neighbour's need it) give every vertex the values of a run
+    without hub vertices, whose aggregation is all in the tiles (the counts to
+    the rounding of the FP64 sum of the tile partials, whose tiles follow each
+    run's tile shapes: shapes tuned earlier in the process for one of the two
+    hub settings are used even without autotuning).  Repeated tuned calls are
+    bit-identical."""
+    for gname in ("rmat10", "rmat12"):
+        _, _, _, col, row = golden.graph(gname)
+        g = sg.DeviceGraph(col, row)
+        for tname in ("tree12", "spider7", "tree5"):
+            t = sg.Graph(*TEMPLATES[tname])
+            for mode in (sg.MODE_REFERENCE, sg.MODE_FP64):
+                a = sg.count(g, t, 3, 5, mode=mode, exact=True, autotune=False, hub_threshold=16)
+                b = sg.count(g, t, 3, 5, mode=mode, exact=True, autotune=False, hub_threshold=0)
+                assert all(rel(x, y) <= 1e-12 for x, y in zip(a, b)), (gname, tname, mode, a, b)
+                c = sg.count(g, t, 3, 5, mode=mode, exact=True, hub_threshold=16)
+                d = sg.count(g, t, 3, 5, mode=mode, exact=True, hub_threshold=16)
+                assert np.array_equal(c, d), (gname, tname, mode, c, d)
+                assert all(rel(x, y) <= 1e-12 for x, y in zip(c, b)), (gname, tname, mode, c, b)
+
+
 def test_countmat_interface(golden):
     c = next(c for c in golden.cases if c.template == "tree5" and c.graph == "rmat10")
     V, s, d, _, _ = golden.graph("rmat10")
