@@ -942,9 +942,9 @@ __device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, unsig
         cp_async_commit();
     }
     plan((NSLOT - 1) * IDS_B);
-    // Step b: copy batch b + NSLOT - 1 (planned by the step before) and fetch
-    // the ids of batch b + 2 NSLOT - 1; wait for batch b + 1 and read it into
-    // registers; plan batch b + NSLOT; add batch b (read by the step before).
+    // Step b: add batch b (read by the step before); copy batch b + NSLOT - 1
+    // (planned by the step before) and fetch the ids of batch b + 2 NSLOT - 1;
+    // wait for batch b + 1 and read it into registers; plan batch b + NSLOT.
     // Steps b < nbt - NSLOT copy and add full batches and have no branch, so
     // that the copies, the shared loads and the plan fill the latency of the
     // add chains; the last NSLOT steps copy what is left of the list and add
@@ -952,6 +952,19 @@ __device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, unsig
     uint32_t ts_b = (NSLOT - 1) * TILE_B, is_b = (NSLOT - 1) * IDS_B, ls_b = TILE_B;
     T acc = T(0);
     auto step = [&](int b, T(&cur)[BR], T(&nxt)[BR], bool tail, bool last) {
+        // the adds of batch b first (its rows are in registers since the step
+        // before): the copies, waits, shared loads and plan of the batches
+        // ahead below are independent of them and fill the latency of the
+        // dependent add chain
+        if (!last) {
+#pragma unroll
+            for (int u = 0; u < BR; ++u) acc = add_rn(acc, cur[u]);
+        } else {
+            const int n = deg - b * BR;
+#pragma unroll
+            for (int u = 0; u < BR; ++u)
+                if (u < n) acc = add_rn(acc, cur[u]);
+        }
         if (!tail) {
 #pragma unroll
             for (int k = 0; k < RPL; ++k)
@@ -968,15 +981,6 @@ __device__ __forceinline__ void hub_item_exact(const HubArgs &h, int item, unsig
         load(nxt, ls_b);              // batch b + 1 (unused past the list)
         ls_b = ls_b == (NSLOT - 1) * TILE_B ? 0 : ls_b + TILE_B;
         plan(is_b);                   // batch b + NSLOT: its ids landed with batch b's rows
-        if (!last) {
-#pragma unroll
-            for (int u = 0; u < BR; ++u) acc = add_rn(acc, cur[u]);
-        } else {
-            const int n = deg - b * BR;
-#pragma unroll
-            for (int u = 0; u < BR; ++u)
-                if (u < n) acc = add_rn(acc, cur[u]);
-        }
     };
     T x[BR], y[BR];
     cp_async_wait<NSLOT - 2>();   // batch 0
